@@ -1,0 +1,925 @@
+/*
+ * euler_oracle.c -- CPU oracle for the 2D Euler finite-volume step.
+ *
+ * TEST INFRASTRUCTURE ONLY (see euler_oracle.h).  A restatement, in its own
+ * structure, of the reference's hot path: per-interface point functions for
+ * the eigenvectors, reconstructions and Riemann fluxes, and grid drivers for
+ * the sweeps, boundaries, flux difference, SSP-RK stages and CFL reduction.
+ * Each function names the reference file:line it follows.  Floating-point
+ * expressions are written in the reference's evaluation order and the file is
+ * compiled without FMA contraction (-ffp-contract=off), so results are
+ * bit-identical to the reference built with gcc -O3.
+ */
+#include "euler_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define AT(a, k, i, j) (a)[((size_t)(k) * rows + (size_t)(i)) * cols + (size_t)(j)]
+
+/* ------------------------------------------------------------------------ */
+/* scalar helpers: include/function.h:28-74                                  */
+/* ------------------------------------------------------------------------ */
+static int sign_of(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+static double larger(double a, double b) { return a > b ? a : b; }
+static double smaller(double a, double b) { return a > b ? b : a; }
+
+/* min_mod, include/function.h:66-68 */
+static double limiter_minmod(double a, double b) {
+    return 0.5 * (sign_of(a) + sign_of(b)) * smaller(fabs(a), fabs(b));
+}
+/* van_leer, include/function.h:71-74 */
+static double limiter_vanleer(double a, double b) {
+    double tiny = 1.0e-6;
+    return ((sign_of(a) + sign_of(b)) * a * b) / (fabs(a) + fabs(b) + tiny);
+}
+
+void orc_defaults(orc_params *p, int nx, int ny) {
+    memset(p, 0, sizeof(*p));
+    p->nx = nx;
+    p->ny = ny;
+    p->gc = 4;
+    p->gamma = 1.4;
+    p->cfl = 0.5;
+    p->recon = 5;
+    p->characteristic = 0;
+    p->weno_z = 1;
+    p->source = 0;
+    p->gravity = 1.0;
+    for (int s = 0; s < 4; s++) p->bc[s] = ORC_BC_OUTFLOW;
+    /* inflow_state and *_fixed_value_state defaults:
+       include/Boundary_Condition.h:49, include/initialize.h:1298-1301 */
+    double mach3[4] = {1.4, 1.4 * 3.0, 0.0, 1.0 / 0.4 + 0.5 * 1.4 * 3.0 * 3.0};
+    for (int k = 0; k < 4; k++) {
+        p->inflow[k] = mach3[k];
+        for (int s = 0; s < 4; s++) p->fixed[s][k] = mach3[k];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* primitive variables: include/initialize.h:1437-1454                      */
+/* ------------------------------------------------------------------------ */
+void orc_con_to_pri(const orc_params *p, const double *U, double *pri) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const double gm1 = p->gamma - 1;
+#pragma omp parallel for
+    for (int i = gc - 1; i <= rows - gc; i++)
+        for (int j = gc - 1; j <= cols - gc; j++) {
+            double r = AT(U, 0, i, j);
+            double u = AT(U, 1, i, j) / AT(U, 0, i, j);
+            double v = AT(U, 2, i, j) / AT(U, 0, i, j);
+            double pr = (AT(U, 3, i, j) - 0.5 * r * (u * u + v * v)) * gm1;
+            AT(pri, 0, i, j) = r;
+            AT(pri, 1, i, j) = u;
+            AT(pri, 2, i, j) = v;
+            AT(pri, 3, i, j) = pr;
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Roe-averaged eigenvectors at one interface between cells a and b.         */
+/* dir 1: include/Characteriz.h:314-392;  dir 2: :416-494.                   */
+/* Lm[k][m] is left-eigenvector row k; Rm[m][k] is the right-eigenvector     */
+/* entry for conserved component m of characteristic field k.                */
+/* ------------------------------------------------------------------------ */
+static void roe_eigen(int dir, const double a[4], const double b[4], double gamma,
+                      double Lm[4][4], double Rm[4][4]) {
+    const double gr = gamma / (gamma - 1);
+    /* enthalpy of each cell, Characteriz.h:319 / :421 */
+    double Ha = 0.5 * (a[1] * a[1] + a[2] * a[2]) + gr * (a[3] / a[0]);
+    double Hb = 0.5 * (b[1] * b[1] + b[2] * b[2]) + gr * (b[3] / b[0]);
+    double D = sqrt(b[0] / a[0]);
+    double D1 = D + 1.0;
+    double u = (a[1] + D * b[1]) / D1;
+    double v = (a[2] + D * b[2]) / D1;
+    double H = (Ha + D * Hb) / D1;
+    double q2 = u * u + v * v;
+    double c2 = (gamma - 1.0) * (H - 0.5 * q2);
+    double c = sqrt(c2);
+    double b1 = (gamma - 1.0) / c2;
+    double b2 = 1.0 + b1 * q2 - b1 * H;
+    if (dir == 1) {
+        Lm[0][0] = 0.5 * (b2 + u / c);
+        Lm[0][1] = -0.5 * (b1 * u + 1.0 / c);
+        Lm[0][2] = -0.5 * b1 * v;
+        Lm[0][3] = 0.5 * b1;
+        Lm[1][0] = -q2 + H;  Lm[1][1] = u;   Lm[1][2] = v;    Lm[1][3] = -1.0;
+        Lm[2][0] = v;        Lm[2][1] = 0.0; Lm[2][2] = -1.0; Lm[2][3] = 0.0;
+        Lm[3][0] = 0.5 * (b2 - u / c);
+        Lm[3][1] = 0.5 * (-b1 * u + 1.0 / c);
+        Lm[3][2] = 0.5 * -b1 * v;
+        Lm[3][3] = 0.5 * b1;
+        Rm[0][0] = 1.0;           Rm[0][1] = b1;          Rm[0][2] = 0.0;  Rm[0][3] = 1.0;
+        Rm[1][0] = u - 1.0 * c;   Rm[1][1] = u * b1;      Rm[1][2] = 0.0;  Rm[1][3] = u + 1.0 * c;
+        Rm[2][0] = v - 0.0 * c;   Rm[2][1] = v * b1;      Rm[2][2] = -1.0; Rm[2][3] = v + 0.0 * c;
+        Rm[3][0] = H - u * c;     Rm[3][1] = H * b1 - 1.0; Rm[3][2] = -v;  Rm[3][3] = H + u * c;
+    } else {
+        Lm[0][0] = 0.5 * (b2 + v / c);
+        Lm[0][1] = -0.5 * (b1 * u + 0.0 / c);
+        Lm[0][2] = -0.5 * (b1 * v + 1.0 / c);
+        Lm[0][3] = 0.5 * b1;
+        Lm[1][0] = -q2 + H;  Lm[1][1] = u;   Lm[1][2] = v;    Lm[1][3] = -1.0;
+        Lm[2][0] = -u;       Lm[2][1] = 1.0; Lm[2][2] = -0.0; Lm[2][3] = 0.0;
+        Lm[3][0] = 0.5 * (b2 - v / c);
+        Lm[3][1] = 0.5 * (-b1 * u + 0.0 / c);
+        Lm[3][2] = 0.5 * (-b1 * v + 1.0 / c);
+        Lm[3][3] = 0.5 * b1;
+        Rm[0][0] = 1.0;           Rm[0][1] = b1;          Rm[0][2] = 0.0;  Rm[0][3] = 1.0;
+        Rm[1][0] = u - 0.0 * c;   Rm[1][1] = u * b1;      Rm[1][2] = 1.0;  Rm[1][3] = u + 0.0 * c;
+        Rm[2][0] = v - 1.0 * c;   Rm[2][1] = v * b1;      Rm[2][2] = -0.0; Rm[2][3] = v + 1.0 * c;
+        Rm[3][0] = H - v * c;     Rm[3][1] = H * b1 - 1.0; Rm[3][2] = u;   Rm[3][3] = H + v * c;
+    }
+}
+
+void orc_eigen(const orc_params *p, int dir, const double *pri, double *eig_l,
+               double *eig_r) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const size_t plane = (size_t)rows * cols;
+    int i0, i1, j0, j1;
+    if (dir == 1) { i0 = gc - 1; i1 = rows - gc; j0 = gc; j1 = cols - gc; }
+    else          { i0 = gc; i1 = rows - gc; j0 = gc - 1; j1 = cols - gc + 1; }
+    for (int i = i0; i < i1; i++)
+        for (int j = j0; j < j1; j++) {
+            double a[4], b[4], Lm[4][4], Rm[4][4];
+            for (int k = 0; k < 4; k++) {
+                a[k] = AT(pri, k, i, j);
+                b[k] = dir == 1 ? AT(pri, k, i + 1, j) : AT(pri, k, i, j + 1);
+            }
+            roe_eigen(dir, a, b, p->gamma, Lm, Rm);
+            for (int k = 0; k < 4; k++)
+                for (int m = 0; m < 4; m++) {
+                    eig_l[(size_t)(k * 4 + m) * plane + (size_t)i * cols + j] = Lm[k][m];
+                    eig_r[(size_t)(m * 4 + k) * plane + (size_t)i * cols + j] = Rm[m][k];
+                }
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* point reconstructions                                                     */
+/* ------------------------------------------------------------------------ */
+/* Jiang-Shu smoothness indicators of a 5-point stencil, as written in
+ * WENO5_L (include/Reconstruction.h:1425-1432). */
+static void smoothness(double v1, double v2, double v3, double v4, double v5,
+                       double *s1, double *s2, double *s3) {
+    *s1 = 13.0 / 12.0 * (v1 - 2.0 * v2 + v3) * (v1 - 2.0 * v2 + v3)
+        + 0.25 * (v1 - 4.0 * v2 + 3.0 * v3) * (v1 - 4.0 * v2 + 3.0 * v3);
+    *s2 = 13.0 / 12.0 * (v2 - 2.0 * v3 + v4) * (v2 - 2.0 * v3 + v4)
+        + 0.25 * (v2 - v4) * (v2 - v4);
+    *s3 = 13.0 / 12.0 * (v3 - 2.0 * v4 + v5) * (v3 - 2.0 * v4 + v5)
+        + 0.25 * (3.0 * v3 - 4.0 * v4 + v5) * (3.0 * v3 - 4.0 * v4 + v5);
+}
+
+/* Weighted sum of the three candidate polynomials (Reconstruction.h:1452-1454). */
+static double blend(double a1, double a2, double a3, double v1, double v2,
+                    double v3, double v4, double v5) {
+    double w1 = a1 / (a1 + a2 + a3);
+    double w2 = a2 / (a1 + a2 + a3);
+    double w3 = a3 / (a1 + a2 + a3);
+    return w1 * (2.0 * v1 - 7.0 * v2 + 11.0 * v3) / 6.0
+         + w2 * (-v2 + 5.0 * v3 + 2.0 * v4) / 6.0
+         + w3 * (2.0 * v3 + 5.0 * v4 - v5) / 6.0;
+}
+
+/* WENO5_L with Jiang-Shu weights (include/Reconstruction.h:1408-1455).  The
+ * right-biased WENO5_R (:1464-1508) is the same with the stencil mirrored. */
+static double weno5_js(double v1, double v2, double v3, double v4, double v5) {
+    const double eps = 1.0e-15;
+    double s1, s2, s3;
+    smoothness(v1, v2, v3, v4, v5, &s1, &s2, &s3);
+    double a1 = 0.1 / (eps + s1) / (eps + s1);
+    double a2 = 0.6 / (eps + s2) / (eps + s2);
+    double a3 = 0.3 / (eps + s3) / (eps + s3);
+    return blend(a1, a2, a3, v1, v2, v3, v4, v5);
+}
+
+/* WENO5Z_L / WENO5Z_R weights (include/Reconstruction.h:1519-1624). */
+static double weno5_z(double v1, double v2, double v3, double v4, double v5) {
+    const double eps = 1.0e-15;
+    double s1, s2, s3;
+    smoothness(v1, v2, v3, v4, v5, &s1, &s2, &s3);
+    double tau = fabs(s1 - s3);
+    double a1 = 0.1 * (1.0 + tau / (s1 + eps));
+    double a2 = 0.6 * (1.0 + tau / (s2 + eps));
+    double a3 = 0.3 * (1.0 + tau / (s3 + eps));
+    return blend(a1, a2, a3, v1, v2, v3, v4, v5);
+}
+
+/* TVD_minmod_L/R and TVD_vanleer_L/R (include/Reconstruction.h:1088-1201):
+ * slopes from a 3-cell stencil centred on c; side +1 gives the value at the
+ * right face of c, side -1 at its left face. */
+static double muscl(double lo, double c, double hi, double delta, int vanleer,
+                    int side) {
+    double s1 = (c - lo) / delta;
+    double s2 = (hi - c) / delta;
+    double s = vanleer ? limiter_vanleer(s1, s2) : limiter_minmod(s1, s2);
+    return side > 0 ? c + 0.5 * s * delta : c - 0.5 * s * delta;
+}
+
+/* interface value pair from a 6-point stencil q[0..5] = cells i-2..i+3 */
+static void recon_pair(int recon, int weno_z, int vanleer, const double q[6],
+                       double delta, double *qm, double *qp) {
+    if (recon == 5) {
+        if (weno_z) {
+            *qm = weno5_z(q[0], q[1], q[2], q[3], q[4]);
+            *qp = weno5_z(q[5], q[4], q[3], q[2], q[1]);
+        } else {
+            *qm = weno5_js(q[0], q[1], q[2], q[3], q[4]);
+            *qp = weno5_js(q[5], q[4], q[3], q[2], q[1]);
+        }
+    } else if (recon == 2) {
+        *qm = muscl(q[1], q[2], q[3], delta, vanleer, +1);
+        *qp = muscl(q[2], q[3], q[4], delta, vanleer, -1);
+    } else { /* first-order Godunov */
+        *qm = q[2];
+        *qp = q[3];
+    }
+}
+
+/* Reconstruction of one sweep: WENO5_Reconstruction (Reconstruction.h:887-1075),
+ * TVD_Reconstruction (:260-446), Reconstruction_Godunov (:51-239).  The
+ * characteristic branch projects the 6-cell stencil with the interface's
+ * left eigenvectors, reconstructs each field, and maps back with the right
+ * eigenvectors, summing fields in order from 0.0 as the reference does. */
+int orc_recon(const orc_params *p, int dir, const double *U, double *conserl,
+              double *conserr, double dx, double dy) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const int recon = p->recon;
+    if (recon != 1 && recon != 2 && recon != 5) return -1;
+    const int ch = p->characteristic;
+    /* characteristic TVD uses van Leer, component TVD uses minmod
+       (Reconstruction.h:314-315, 418-419); WENO-Z is used only by the
+       characteristic WENO5 branch (:941-942 vs :1048-1049). */
+    const int vanleer = ch;
+    const int wz = ch && p->weno_z;
+    const double delta = dir == 1 ? dx : dy;
+    double *pri = NULL;
+    if (ch) {
+        pri = (double *)calloc((size_t)4 * rows * cols, sizeof(double));
+        if (!pri) return -2;
+        orc_con_to_pri(p, U, pri);
+    }
+    int i0, i1, j0, j1;
+    if (dir == 1) { i0 = gc - 1; i1 = rows - gc; j0 = gc; j1 = cols - gc; }
+    else          { i0 = gc; i1 = rows - gc; j0 = gc - 1; j1 = cols - gc; }
+#pragma omp parallel for
+    for (int i = i0; i < i1; i++)
+        for (int j = j0; j < j1; j++) {
+            if (!ch) {
+                for (int k = 0; k < 4; k++) {
+                    double q[6];
+                    for (int n = 0; n < 6; n++)
+                        q[n] = dir == 1 ? AT(U, k, i - 2 + n, j) : AT(U, k, i, j - 2 + n);
+                    double qm, qp;
+                    recon_pair(recon, 0, 0, q, delta, &qm, &qp);
+                    AT(conserl, k, i, j) = qm;
+                    AT(conserr, k, i, j) = qp;
+                }
+                continue;
+            }
+            double a[4], b[4], Lm[4][4], Rm[4][4], wm[4], wp[4];
+            for (int k = 0; k < 4; k++) {
+                a[k] = AT(pri, k, i, j);
+                b[k] = dir == 1 ? AT(pri, k, i + 1, j) : AT(pri, k, i, j + 1);
+            }
+            roe_eigen(dir, a, b, p->gamma, Lm, Rm);
+            for (int k = 0; k < 4; k++) {
+                double q[6];
+                for (int n = 0; n < 6; n++) {
+                    int ii = dir == 1 ? i - 2 + n : i, jj = dir == 1 ? j : j - 2 + n;
+                    double acc = 0.0;
+                    for (int m = 0; m < 4; m++) acc += AT(U, m, ii, jj) * Lm[k][m];
+                    q[n] = acc;
+                }
+                if (recon == 1) {
+                    /* Godunov projects cells i and i+1 only (Reconstruction.h:96-105) */
+                    wm[k] = q[2];
+                    wp[k] = q[3];
+                } else {
+                    recon_pair(recon, wz, vanleer, q, delta, &wm[k], &wp[k]);
+                }
+            }
+            for (int m = 0; m < 4; m++) {
+                double sl = 0.0, sr = 0.0;
+                for (int k = 0; k < 4; k++) {
+                    sl += wm[k] * Rm[m][k];
+                    sr += wp[k] * Rm[m][k];
+                }
+                AT(conserl, m, i, j) = sl;
+                AT(conserr, m, i, j) = sr;
+            }
+        }
+    free(pri);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Riemann fluxes at one interface.  ql/qr are conserved states; n selects   */
+/* the normal direction (1 = x, 2 = y).  Returns 0, or 1 when HLL skipped     */
+/* the interface (HLL_Flux `continue` on bad states, scheme.h:427-436, 500). */
+/* ------------------------------------------------------------------------ */
+struct side { double r, ru, rv, re, ir, u, v, uu, vv, p; };
+
+static void unpack(const double q[4], double gm1, struct side *s) {
+    s->r = q[0]; s->ru = q[1]; s->rv = q[2]; s->re = q[3];
+    s->ir = 1.0 / s->r;
+    s->u = s->ru * s->ir;
+    s->v = s->rv * s->ir;
+    s->uu = s->u * s->u;
+    s->vv = s->v * s->v;
+    s->p = (s->re - 0.5 * s->r * (s->uu + s->vv)) * gm1;
+}
+
+/* HLLC_Flux, include/scheme.h:690-1001 (x: :702-857, y: :863-998) */
+static void flux_hllc(int n, const double ql[4], const double qr[4], double gamma,
+                      double F[4]) {
+    const double gm1 = gamma - 1.0, gr = gamma / gm1;
+    struct side Ls, Rs;
+    unpack(ql, gm1, &Ls);
+    unpack(qr, gm1, &Rs);
+    double aL, aR, HL, HR;
+    if (n == 1) {
+        HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+        HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+        aL = sqrt((gamma - 1.0) * (HL - 0.5 * (Ls.uu + Ls.vv)));
+        aR = sqrt((gamma - 1.0) * (HR - 0.5 * (Rs.uu + Rs.vv)));
+    } else {
+        aL = sqrt(gamma * Ls.p * Ls.ir);
+        aR = sqrt(gamma * Rs.p * Rs.ir);
+        HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+        HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    }
+    /* normal (un) and tangential (ut) velocities, physical fluxes */
+    double unL = n == 1 ? Ls.u : Ls.v, unR = n == 1 ? Rs.u : Rs.v;
+    double FL[4], FR[4];
+    if (n == 1) {
+        FL[0] = Ls.r * Ls.u; FR[0] = Rs.r * Rs.u;
+        FL[1] = Ls.r * Ls.uu + Ls.p; FR[1] = Rs.r * Rs.uu + Rs.p;
+        FL[2] = Ls.r * Ls.v * Ls.u; FR[2] = Rs.r * Rs.v * Rs.u;
+        FL[3] = Ls.r * HL * Ls.u; FR[3] = Rs.r * HR * Rs.u;
+    } else {
+        FL[0] = Ls.r * Ls.v; FR[0] = Rs.r * Rs.v;
+        FL[1] = Ls.r * Ls.u * Ls.v; FR[1] = Rs.r * Rs.u * Rs.v;
+        FL[2] = Ls.r * Ls.vv + Ls.p; FR[2] = Rs.r * Rs.vv + Rs.p;
+        FL[3] = Ls.r * HL * Ls.v; FR[3] = Rs.r * HR * Rs.v;
+    }
+    double sqL = sqrt(Ls.r), sqR = sqrt(Rs.r);
+    double ssum = sqL + sqR;
+    double isum = 1.0 / ssum;
+    double ubar = (sqL * Ls.u + sqR * Rs.u) * isum;
+    double vbar = (sqL * Ls.v + sqR * Rs.v) * isum;
+    double eta = n == 1 ? 0.5 * sqL * sqR * isum * isum
+                        : 0.5 * sqL * sqR / (ssum * ssum);
+    double dun = unR - unL;
+    double dd = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun);
+    double nbar = n == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    double denom = Ls.r * (sl - unL) - Rs.r * (sr - unR);
+    double ss = (Rs.p - Ls.p + Ls.r * unL * (sl - unL) - Rs.r * unR * (sr - unR)) / denom;
+    double mL = Ls.r * (sl - unL) / (sl - ss);
+    double mR = Rs.r * (sr - unR) / (sr - ss);
+    double eL = Ls.re * Ls.ir + (ss - unL) * (ss + Ls.p / (Ls.r * (sl - unL)));
+    double eR = Rs.re * Rs.ir + (ss - unR) * (ss + Rs.p / (Rs.r * (sr - unR)));
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    } else if (ss >= 0.0) {
+        F[0] = FL[0] + sl * (mL - Ls.r);
+        if (n == 1) {
+            F[1] = FL[1] + sl * (mL * ss - Ls.ru);
+            F[2] = FL[2] + sl * (mL * Ls.v - Ls.rv);
+        } else {
+            F[1] = FL[1] + sl * (mL * Ls.u - Ls.ru);
+            F[2] = FL[2] + sl * (mL * ss - Ls.rv);
+        }
+        F[3] = FL[3] + sl * (mL * eL - Ls.re);
+    } else {
+        F[0] = FR[0] + sr * (mR - Rs.r);
+        if (n == 1) {
+            F[1] = FR[1] + sr * (mR * ss - Rs.ru);
+            F[2] = FR[2] + sr * (mR * Rs.v - Rs.rv);
+        } else {
+            F[1] = FR[1] + sr * (mR * Rs.u - Rs.ru);
+            F[2] = FR[2] + sr * (mR * ss - Rs.rv);
+        }
+        F[3] = FR[3] + sr * (mR * eR - Rs.re);
+    }
+}
+
+/* HLL_Flux, include/scheme.h:400-674 */
+static int flux_hll(int n, const double ql[4], const double qr[4], double gamma,
+                    double F[4]) {
+    if (ql[0] <= 0.0 || qr[0] <= 0.0) return 1;
+    if (isnan(ql[0]) || isnan(qr[0])) return 1;
+    struct side Ls, Rs;
+    unpack(ql, gamma - 1.0, &Ls);
+    unpack(qr, gamma - 1.0, &Rs);
+    double gr = gamma / (gamma - 1.0);
+    double HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+    double HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    double aL = sqrt((gamma - 1.0) * (HL - 0.5 * (Ls.uu + Ls.vv)));
+    double aR = sqrt((gamma - 1.0) * (HR - 0.5 * (Rs.uu + Rs.vv)));
+    double FL[4], FR[4];
+    if (n == 1) {
+        FL[0] = Ls.r * Ls.u; FR[0] = Rs.r * Rs.u;
+        FL[1] = Ls.r * Ls.uu + Ls.p; FR[1] = Rs.r * Rs.uu + Rs.p;
+        FL[2] = Ls.r * Ls.v * Ls.u; FR[2] = Rs.r * Rs.v * Rs.u;
+        FL[3] = Ls.r * HL * Ls.u; FR[3] = Rs.r * HR * Rs.u;
+    } else {
+        FL[0] = Ls.r * Ls.v; FR[0] = Rs.r * Rs.v;
+        FL[1] = Ls.r * Ls.u * Ls.v; FR[1] = Rs.r * Rs.u * Rs.v;
+        FL[2] = Ls.r * Ls.vv + Ls.p; FR[2] = Rs.r * Rs.vv + Rs.p;
+        FL[3] = Ls.r * HL * Ls.v; FR[3] = Rs.r * HR * Rs.v;
+    }
+    double sqL = sqrt(Ls.r), sqR = sqrt(Rs.r);
+    double ssum = sqL + sqR;
+    double isum = 1.0 / ssum;
+    double ubar = (sqL * Ls.u + sqR * Rs.u) * isum;
+    double vbar = (sqL * Ls.v + sqR * Rs.v) * isum;
+    double eta = 0.5 * sqL * sqR / (ssum * ssum);
+    double dun = n == 1 ? Rs.u - Ls.u : Rs.v - Ls.v;
+    double dd = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun);
+    if (isnan(dd)) return 1;
+    double nbar = n == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    const double UL[4] = {Ls.r, Ls.ru, Ls.rv, Ls.re}, UR[4] = {Rs.r, Rs.ru, Rs.rv, Rs.re};
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    } else {
+        double idiff = 1.0 / (sr - sl);
+        double slsr = sl * sr;
+        for (int k = 0; k < 4; k++)
+            F[k] = (sr * FL[k] - sl * FR[k] + slsr * (UR[k] - UL[k])) * idiff;
+    }
+    return 0;
+}
+
+/* Roe_Flux, include/scheme.h:1018-1322 (no-op entropy fix at :1117-1126) */
+static void flux_roe(int n, const double ql[4], const double qr[4], double gamma,
+                     double F[4]) {
+    const double gm1 = gamma - 1.0, gr = gamma / gm1;
+    struct side Ls, Rs;
+    unpack(ql, gm1, &Ls);
+    unpack(qr, gm1, &Rs);
+    double HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+    double HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    double FL[4], FR[4];
+    if (n == 1) {
+        FL[0] = Ls.r * Ls.u; FR[0] = Rs.r * Rs.u;
+        FL[1] = Ls.r * Ls.uu + Ls.p; FR[1] = Rs.r * Rs.uu + Rs.p;
+        FL[2] = Ls.r * Ls.v * Ls.u; FR[2] = Rs.r * Rs.v * Rs.u;
+        FL[3] = Ls.r * HL * Ls.u; FR[3] = Rs.r * HR * Rs.u;
+    } else {
+        FL[0] = Ls.r * Ls.v; FR[0] = Rs.r * Rs.v;
+        FL[1] = Ls.r * Ls.u * Ls.v; FR[1] = Rs.r * Rs.u * Rs.v;
+        FL[2] = Ls.r * Ls.vv + Ls.p; FR[2] = Rs.r * Rs.vv + Rs.p;
+        FL[3] = Ls.r * HL * Ls.v; FR[3] = Rs.r * HR * Rs.v;
+    }
+    double sqL = sqrt(Ls.r), sqR = sqrt(Rs.r);
+    double isum = 1.0 / (sqL + sqR);
+    double rbar = sqL * sqR;
+    double ubar = (sqL * Ls.u + sqR * Rs.u) * isum;
+    double vbar = (sqL * Ls.v + sqR * Rs.v) * isum;
+    double Hbar = (sqL * HL + sqR * HR) * isum;
+    double q2 = ubar * ubar + vbar * vbar;
+    double cbar = sqrt(gm1 * (Hbar - 0.5 * q2));
+    double nbar = n == 1 ? ubar : vbar;
+    double lam[4] = {fabs(nbar - cbar), fabs(nbar), fabs(nbar), fabs(nbar + cbar)};
+    double drho = Rs.r - Ls.r, du = Rs.u - Ls.u, dv = Rs.v - Ls.v, dp = Rs.p - Ls.p;
+    double c2 = cbar * cbar;
+    double i2c2 = 1.0 / (2.0 * c2);
+    double ic2 = 1.0 / c2;
+    double dn = n == 1 ? du : dv, dt_ = n == 1 ? dv : du;
+    double al[4];
+    al[0] = (dp - rbar * cbar * dn) * i2c2;
+    al[1] = drho - dp * ic2;
+    al[2] = rbar * dt_;
+    al[3] = (dp + rbar * cbar * dn) * i2c2;
+    double K[4][4];
+    if (n == 1) {
+        double k0[4] = {1.0, ubar - cbar, vbar, Hbar - ubar * cbar};
+        double k1[4] = {1.0, ubar, vbar, 0.5 * q2};
+        double k2[4] = {0.0, 0.0, 1.0, vbar};
+        double k3[4] = {1.0, ubar + cbar, vbar, Hbar + ubar * cbar};
+        memcpy(K[0], k0, sizeof k0); memcpy(K[1], k1, sizeof k1);
+        memcpy(K[2], k2, sizeof k2); memcpy(K[3], k3, sizeof k3);
+    } else {
+        double k0[4] = {1.0, ubar, vbar - cbar, Hbar - vbar * cbar};
+        double k1[4] = {1.0, ubar, vbar, 0.5 * q2};
+        double k2[4] = {0.0, 1.0, 0.0, ubar};
+        double k3[4] = {1.0, ubar, vbar + cbar, Hbar + vbar * cbar};
+        memcpy(K[0], k0, sizeof k0); memcpy(K[1], k1, sizeof k1);
+        memcpy(K[2], k2, sizeof k2); memcpy(K[3], k3, sizeof k3);
+    }
+    for (int c = 0; c < 4; c++) F[c] = 0.5 * (FL[c] + FR[c]);
+    for (int w = 0; w < 4; w++) {
+        double term = 0.5 * lam[w] * al[w];
+        for (int c = 0; c < 4; c++) F[c] -= term * K[w][c];
+    }
+}
+
+/* LLF_Flux, include/scheme.h:229-381 (the dispatch default) */
+static void flux_llf(int n, const double ql[4], const double qr[4], double gamma,
+                     double F[4]) {
+    const double gm1 = gamma - 1.0, gr = gamma / gm1;
+    struct side Ls, Rs;
+    unpack(ql, gm1, &Ls);
+    unpack(qr, gm1, &Rs);
+    double aL = sqrt(gamma * Ls.p * Ls.ir), aR = sqrt(gamma * Rs.p * Rs.ir);
+    double HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+    double HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    double FL[4], FR[4];
+    if (n == 1) {
+        FL[0] = Ls.r * Ls.u; FR[0] = Rs.r * Rs.u;
+        FL[1] = Ls.r * Ls.uu + Ls.p; FR[1] = Rs.r * Rs.uu + Rs.p;
+        FL[2] = Ls.r * Ls.v * Ls.u; FR[2] = Rs.r * Rs.v * Rs.u;
+        FL[3] = Ls.r * HL * Ls.u; FR[3] = Rs.r * HR * Rs.u;
+    } else {
+        FL[0] = Ls.r * Ls.v; FR[0] = Rs.r * Rs.v;
+        FL[1] = Ls.r * Ls.u * Ls.v; FR[1] = Rs.r * Rs.u * Rs.v;
+        FL[2] = Ls.r * Ls.vv + Ls.p; FR[2] = Rs.r * Rs.vv + Rs.p;
+        FL[3] = Ls.r * HL * Ls.v; FR[3] = Rs.r * HR * Rs.v;
+    }
+    double unL = n == 1 ? Ls.u : Ls.v, unR = n == 1 ? Rs.u : Rs.v;
+    double sp = larger(fabs(unL) + aL, fabs(unR) + aR);
+    const double UL[4] = {Ls.r, Ls.ru, Ls.rv, Ls.re}, UR[4] = {Rs.r, Rs.ru, Rs.rv, Rs.re};
+    for (int k = 0; k < 4; k++) F[k] = 0.5 * (FL[k] + FR[k]) - 0.5 * sp * (UR[k] - UL[k]);
+}
+
+static int point_flux(int scheme, int n, const double ql[4], const double qr[4],
+                      double gamma, double F[4]) {
+    switch (scheme) {
+        case 1: return flux_hll(n, ql, qr, gamma, F);
+        case 2: flux_hllc(n, ql, qr, gamma, F); return 0;
+        case 3: flux_roe(n, ql, qr, gamma, F); return 0;
+        default: flux_llf(n, ql, qr, gamma, F); return 0;
+    }
+}
+
+void orc_riemann(const orc_params *p, int scheme, int dir, const double *ql,
+                 const double *qr, double *flux) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    int i0, i1, j0, j1;
+    if (dir == 1) { i0 = gc - 1; i1 = rows - gc; j0 = gc; j1 = cols - gc; }
+    else          { i0 = gc; i1 = rows - gc; j0 = gc - 1; j1 = cols - gc; }
+#pragma omp parallel for
+    for (int i = i0; i < i1; i++)
+        for (int j = j0; j < j1; j++) {
+            double a[4], b[4], F[4];
+            for (int k = 0; k < 4; k++) { a[k] = AT(ql, k, i, j); b[k] = AT(qr, k, i, j); }
+            if (point_flux(scheme, dir, a, b, p->gamma, F) == 0)
+                for (int k = 0; k < 4; k++) AT(flux, k, i, j) = F[k];
+        }
+}
+
+int orc_flux_recon(const orc_params *p, int scheme, const double *U, double *f,
+                   double *g, double dx, double dy) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const size_t n = (size_t)4 * rows * cols;
+    double *ql = (double *)malloc(n * sizeof(double));
+    double *qr = (double *)malloc(n * sizeof(double));
+    if (!ql || !qr) { free(ql); free(qr); return -2; }
+    int rc = orc_recon(p, 1, U, ql, qr, dx, dy);
+    if (rc == 0) {
+        orc_riemann(p, scheme, 1, ql, qr, f);
+        rc = orc_recon(p, 2, U, ql, qr, dx, dy);
+    }
+    if (rc == 0) orc_riemann(p, scheme, 2, ql, qr, g);
+    free(ql);
+    free(qr);
+    return rc;
+}
+
+void orc_space_item(const orc_params *p, double dx, double dy, const double *f,
+                    const double *g, const double *s, double *Lout) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const double idx = 1.0 / dx, idy = 1.0 / dy;
+#pragma omp parallel for
+    for (int i = gc; i <= rows - gc - 1; i++)
+        for (int j = gc; j <= cols - gc - 1; j++)
+            for (int k = 0; k < 4; k++)
+                AT(Lout, k, i, j) = -(AT(f, k, i, j) - AT(f, k, i - 1, j)) * idx
+                                  - (AT(g, k, i, j) - AT(g, k, i, j - 1)) * idy
+                                  + AT(s, k, i, j);
+}
+
+void orc_source(const orc_params *p, const double *U, double *s) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    for (int i = gc; i <= rows - gc - 1; i++)
+        for (int j = gc; j <= cols - gc - 1; j++) {
+            double r = AT(U, 0, i, j);
+            double v = AT(U, 2, i, j) / r;
+            AT(s, 0, i, j) = 0.0;
+            AT(s, 1, i, j) = 0.0;
+            AT(s, 2, i, j) = r * p->gravity;
+            AT(s, 3, i, j) = r * p->gravity * v;
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* boundaries: include/Boundary_Condition.h                                  */
+/* ------------------------------------------------------------------------ */
+/* One side of Boundary_Conditions.  side: 0 left, 1 right, 2 bottom, 3 top.
+ * Index ranges (inclusive/exclusive) follow each BC_* routine. */
+static void bc_side(const orc_params *p, double *U, int side) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const int kind = p->bc[side];
+    const int along_j = side < 2;                  /* L/R walk j, B/T walk i */
+    const int lo = gc;
+    int hi = along_j ? cols - gc : rows - gc;      /* exclusive */
+    if (kind == ORC_BC_OUTFLOW) hi += 1;           /* BC_OutFlow_2D uses <= (:223) */
+    const int normal = along_j ? 1 : 2;            /* momentum reversed by walls */
+    for (int k = 0; k < 4; k++)
+        for (int t = lo; t < hi; t++)
+            for (int m = 0; m < 4; m++) {
+                /* ghost index g and its source index src along the normal */
+                int gi, src = -1;
+                double cval = 0.0, sgn = 1.0;
+                int n_int = along_j ? p->nx : p->ny;
+                int nlen = along_j ? rows : cols;
+                (void)n_int;
+                if (side == 0 || side == 2) gi = gc - 1 - m;
+                else gi = nlen - gc + m;
+                switch (kind) {
+                    case ORC_BC_OUTFLOW:
+                        src = (side == 0 || side == 2) ? gc : nlen - gc - 1;
+                        break;
+                    case ORC_BC_PERIODIC:
+                        src = (side == 0 || side == 2) ? nlen - gc - 1 - m : gc + m;
+                        break;
+                    case ORC_BC_REFLECT:
+                        /* left/top mirror four layers (:356-374, :443-461);
+                           right/bottom copy the wall cell (:393-407, :427-441) */
+                        if (side == 0) src = gc + m;
+                        else if (side == 3) src = nlen - gc - 1 - m;
+                        else if (side == 1) src = nlen - gc - 1;
+                        else src = gc;
+                        if (k == normal) sgn = -1.0;
+                        break;
+                    case ORC_BC_INFLOW:
+                        cval = p->inflow[k];
+                        break;
+                    default: /* ORC_BC_FIXED */
+                        cval = p->fixed[side][k];
+                        break;
+                }
+                double val;
+                if (src >= 0) {
+                    double sv = along_j ? AT(U, k, src, t) : AT(U, k, t, src);
+                    val = sgn < 0 ? -sv : sv;
+                } else {
+                    val = cval;
+                }
+                if (along_j) AT(U, k, gi, t) = val;
+                else AT(U, k, t, gi) = val;
+            }
+}
+
+/* BC_DoubleMach_2D, include/Boundary_Condition.h:480-692 */
+static void bc_double_mach(const orc_params *p, double *U, double time) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const double lx = 4.0, ly = 1.0, slope = sqrt(3.0), x0 = 1.0 / 6.0, g = 1.4;
+    const double post[4] = {8.0, 8.0 * 7.1447, 8.0 * -4.125,
+                            116.5 / (g - 1.0) + 0.5 * 8.0 * (7.1447 * 7.1447 + -4.125 * -4.125)};
+    const double pre[4] = {1.4, 1.4 * 0.0, 1.4 * 0.0,
+                           1.0 / (g - 1.0) + 0.5 * 1.4 * (0.0 * 0.0 + 0.0 * 0.0)};
+    const double nx = rows - 2 * gc;
+    for (int j = gc; j < cols - gc; j++)
+        for (int m = 0; m < 4; m++)
+            for (int k = 0; k < 4; k++) AT(U, k, gc - 1 - m, j) = post[k];
+    for (int k = 0; k < 4; k++)
+        for (int j = gc; j < cols - gc; j++)
+            for (int m = 0; m < 4; m++) AT(U, k, rows - gc + m, j) = AT(U, k, rows - gc - 1, j);
+    for (int i = gc; i < rows - gc; i++) {
+        double xp = (double)(i + 0.5 - gc) / nx * lx;
+        for (int m = 0; m < 4; m++)
+            for (int k = 0; k < 4; k++) {
+                if (xp > x0) {
+                    double sv = AT(U, k, i, gc + m);
+                    AT(U, k, i, gc - 1 - m) = k == 2 ? -sv : sv;
+                } else {
+                    AT(U, k, i, gc - 1 - m) = post[k];
+                }
+            }
+    }
+    double xs = x0 + (ly / slope) + (20.0 * time / slope);
+    for (int i = gc; i < rows - gc; i++) {
+        double xp = (double)(i + 0.5 - gc) / nx * lx;
+        for (int m = 0; m < 4; m++)
+            for (int k = 0; k < 4; k++) AT(U, k, i, cols - gc + m) = xp < xs ? post[k] : pre[k];
+    }
+}
+
+void orc_bc(const orc_params *p, double *U, double time) {
+    if (p->dmr) { bc_double_mach(p, U, time); return; }
+    for (int side = 0; side < 4; side++) bc_side(p, U, side);
+}
+
+/* ------------------------------------------------------------------------ */
+/* time integration: include/time_advance.h:643-882                          */
+/* ------------------------------------------------------------------------ */
+int orc_rk(const orc_params *p, int order, int scheme, double *U, double dt,
+           double dx, double dy, double time) {
+    if (order < 1 || order > 3) return -1;
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const size_t n = (size_t)4 * rows * cols;
+    double *buf = (double *)calloc(5 * n, sizeof(double));
+    if (!buf) return -2;
+    double *f = buf, *g = buf + n, *s = buf + 2 * n, *Lt = buf + 3 * n, *U1 = buf + 4 * n;
+    double *U2 = NULL;
+    if (order == 3) {
+        U2 = (double *)calloc(n, sizeof(double));
+        if (!U2) { free(buf); return -2; }
+    }
+    int rc = 0;
+    /* stage inputs and the combination applied after each stage */
+    double *in[3] = {U, U1, U2};
+    for (int st = 0; st < order && rc == 0; st++) {
+        double *x = in[st];
+        if (p->source) orc_source(p, x, s);
+        orc_bc(p, x, time);
+        rc = orc_flux_recon(p, scheme, x, f, g, dx, dy);
+        if (rc) break;
+        orc_space_item(p, dx, dy, f, g, s, Lt);
+#pragma omp parallel for
+        for (int i = gc; i <= rows - gc - 1; i++)
+            for (int j = gc; j <= cols - gc - 1; j++)
+                for (int k = 0; k < 4; k++) {
+                    double y = AT(U, k, i, j), l = AT(Lt, k, i, j);
+                    if (order == 1) {
+                        AT(U, k, i, j) = y + dt * l;
+                    } else if (st == 0) {
+                        AT(U1, k, i, j) = y + dt * l;
+                    } else if (order == 2) {
+                        AT(U, k, i, j) = 0.5 * y + 0.5 * (AT(U1, k, i, j) + dt * l);
+                    } else if (st == 1) {
+                        AT(U2, k, i, j) = (3.0 / 4.0) * y + (1.0 / 4.0) * (AT(U1, k, i, j) + dt * l);
+                    } else {
+                        AT(U, k, i, j) = (1.0 / 3.0) * y + (2.0 / 3.0) * (AT(U2, k, i, j) + dt * l);
+                    }
+                }
+    }
+    free(U2);
+    free(buf);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CFL time step: include/function.h:144-175                                 */
+/* ------------------------------------------------------------------------ */
+void orc_wave_speeds(const orc_params *p, const double *U, double *sx, double *sy) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    double mx = 0.0, my = 0.0;
+    for (int i = gc; i < rows - gc; i++)
+        for (int j = gc; j < cols - gc; j++) {
+            double r = AT(U, 0, i, j);
+            double u = AT(U, 1, i, j) / r;
+            double v = AT(U, 2, i, j) / r;
+            double pr = (AT(U, 3, i, j) - 0.5 * r * (u * u + v * v)) * (p->gamma - 1);
+            double a = sqrt(p->gamma * pr / r);
+            double lx = fabs(u) + a, ly = fabs(v) + a;
+            if (lx > mx) mx = lx;
+            if (ly > my) my = ly;
+        }
+    *sx = mx;
+    *sy = my;
+}
+
+double orc_dt(const orc_params *p, const double *U, double dx, double dy) {
+    double sx, sy;
+    orc_wave_speeds(p, U, &sx, &sy);
+    return p->cfl * smaller(dx, dy) / (sx + sy);
+}
+
+void orc_mesh(int nx, int ny, double *mx, double *my, double dx, double dy) {
+    for (int j = 0; j < nx; j++) mx[j] = dx * j + 0.5 * dx;
+    for (int k = 0; k < ny; k++) my[k] = dy * k + 0.5 * dy;
+}
+
+/* ------------------------------------------------------------------------ */
+/* initial states                                                            */
+/* ------------------------------------------------------------------------ */
+/* initEulerconser2D, include/initialize.h:1389-1405, over the whole array */
+static void prim_to_cons(const orc_params *p, const double *W, double *U) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    for (int i = 0; i < rows; i++)
+        for (int j = 0; j < cols; j++) {
+            double r = AT(W, 0, i, j), u = AT(W, 1, i, j), v = AT(W, 2, i, j), pr = AT(W, 3, i, j);
+            AT(U, 0, i, j) = r;
+            AT(U, 1, i, j) = u * r;
+            AT(U, 2, i, j) = v * r;
+            AT(U, 3, i, j) = pr / (p->gamma - 1) + 0.5 * r * (u * u + v * v);
+        }
+}
+
+int orc_init_case(orc_params *p, int which, const double *q, double *U,
+                  double *lx, double *ly, double *tmax) {
+    const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
+    const size_t n = (size_t)4 * rows * cols;
+    double *W = (double *)calloc(n, sizeof(double));
+    if (!W) return -2;
+    p->dmr = 0;
+    switch (which) {
+        case ORC_CASE_FOUR_QUADRANT: {
+            /* states ordered upper-right, upper-left, lower-left, lower-right */
+            static const double base[16] = {1.5, 0.0, 0.0, 1.5,     0.5323, 1.206, 0.0, 0.3,
+                                             0.138, 1.206, 1.206, 0.029, 0.5323, 0.0, 1.206, 0.3};
+            const double *st = q ? q : base;
+            for (int s = 0; s < 4; s++) p->bc[s] = ORC_BC_OUTFLOW;
+            *lx = 1.0; *ly = 1.0; *tmax = 0.3;
+            for (int i = gc; i < rows - gc; i++)
+                for (int j = gc; j < cols - gc; j++) {
+                    int right = 2 * (i - gc) + 1 >= p->nx, upper = 2 * (j - gc) + 1 >= p->ny;
+                    int qd = upper ? (right ? 0 : 1) : (right ? 3 : 2);
+                    for (int k = 0; k < 4; k++) AT(W, k, i, j) = st[4 * qd + k];
+                }
+            break;
+        }
+        case ORC_CASE_WALL_HEATING: {
+            double speed = q ? q[0] : 1.0;
+            p->bc[0] = ORC_BC_REFLECT; p->bc[1] = ORC_BC_OUTFLOW;
+            p->bc[2] = ORC_BC_PERIODIC; p->bc[3] = ORC_BC_PERIODIC;
+            *lx = 1.0; *ly = 0.02; *tmax = 0.6;
+            for (int i = gc; i < rows - gc; i++)
+                for (int j = gc; j < cols - gc; j++) {
+                    AT(W, 0, i, j) = 1.0; AT(W, 1, i, j) = -speed;
+                    AT(W, 2, i, j) = 0.0; AT(W, 3, i, j) = 1.0e-4;
+                }
+            break;
+        }
+        case ORC_CASE_DOUBLE_MACH: {
+            /* initEulerpri2D_DoubleMachReflection, include/initialize.h:890-952 */
+            const double post[4] = {8.0, 7.1447, -4.125, 116.5}, pre[4] = {1.4, 0.0, 0.0, 1.0};
+            const double slope = sqrt(3.0), x0 = 1.0 / 6.0;
+            *lx = 4.0; *ly = 1.0; *tmax = 0.2;
+            p->dmr = 1;
+            double nxd = rows - 2 * gc, nyd = cols - 2 * gc;
+            for (int i = gc; i < rows - gc; i++)
+                for (int j = gc; j < cols - gc; j++) {
+                    double xp = (double)(i + 0.5 - gc) / nxd * (*lx);
+                    double yp = (double)(j + 0.5 - gc) / nyd * (*ly);
+                    const double *st = yp < slope * (xp - x0) ? pre : post;
+                    for (int k = 0; k < 4; k++) AT(W, k, i, j) = st[k];
+                }
+            break;
+        }
+        case ORC_CASE_PRECISION: {
+            /* initEulerpri1D_PrecisionTest, include/initialize.h:36-60 */
+            p->bc[0] = ORC_BC_PERIODIC; p->bc[1] = ORC_BC_PERIODIC;
+            p->bc[2] = ORC_BC_OUTFLOW; p->bc[3] = ORC_BC_OUTFLOW;
+            *lx = 2.0 * M_PI; *ly = 1.0; *tmax = 2.0;
+            double dx = *lx / (rows - 2 * gc);
+            for (int i = gc; i < rows - gc; i++) {
+                AT(W, 0, i, gc) = 1.0 + 0.2 * sin((i - gc + 0.5) * dx);
+                AT(W, 1, i, gc) = 1.0;
+                AT(W, 2, i, gc) = 0.0;
+                AT(W, 3, i, gc) = 1.0;
+            }
+            break;
+        }
+        case ORC_CASE_NOH_1D:
+        case ORC_CASE_SOD_1D: {
+            /* initEulerpri1D_NohProblem (:315-347), initEulerpri1D_Shocktube (:70-110):
+               these fill the whole array, ghosts included */
+            int noh = which == ORC_CASE_NOH_1D;
+            p->bc[0] = noh ? ORC_BC_REFLECT : ORC_BC_OUTFLOW;
+            p->bc[1] = ORC_BC_OUTFLOW; p->bc[2] = ORC_BC_OUTFLOW; p->bc[3] = ORC_BC_OUTFLOW;
+            *lx = 1.0; *ly = 1.0; *tmax = noh ? 0.6 : 0.2;
+            for (int i = 0; i < rows; i++)
+                for (int j = 0; j < cols; j++) {
+                    double st[4];
+                    if (noh) { st[0] = 1.0; st[1] = -1.0; st[2] = 0.0; st[3] = 1e-6; }
+                    else if (i < rows / 2) { st[0] = 1.0; st[1] = 0.0; st[2] = 0.0; st[3] = 1.0; }
+                    else { st[0] = 0.125; st[1] = 0.0; st[2] = 0.0; st[3] = 0.1; }
+                    for (int k = 0; k < 4; k++) AT(W, k, i, j) = st[k];
+                }
+            break;
+        }
+        default:
+            free(W);
+            return -1;
+    }
+    prim_to_cons(p, W, U);
+    free(W);
+    return 0;
+}
+
+long orc_run(const orc_params *p, int order, int scheme, double *U, double dx,
+             double dy, double tmax, int n_out, double *t_final) {
+    double out_dt = tmax / n_out, next_out = out_dt, dt = 0.0, t;
+    long ite = 0;
+    for (t = 0.0; t < tmax; t = t + dt) {
+        dt = orc_dt(p, U, dx, dy);
+        if (t + dt > next_out) dt = next_out - t;
+        if (t + dt >= tmax) dt = tmax - t;
+        if (orc_rk(p, order, scheme, U, dt, dx, dy, t)) return -1;
+        double now = t + dt;
+        if (fabs(now - next_out) < 1e-10 * out_dt) next_out += out_dt;
+        ite++;
+    }
+    if (t_final) *t_final = t;
+    return ite;
+}
