@@ -1,0 +1,314 @@
+"""Benchmark of the 2D Euler FVM step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step = one SSP-RK3 step of the whole grid, CFL time step from the
+device reduction): the four-quadrant Riemann problem on [0,1]^2, 1024 x 1024
+cells, gamma 1.4, characteristic WENO5-JS + HLLC + SSP-RK3, CFL 0.5, plain
+FP64 drop-in form (bit-identical to the reference).  Inputs are synthetic (the
+benchmark's own initial state); nothing is downloaded.
+
+Our arm prints one JSON line with
+  value     cell-updates/s over all ranks, device time (CUDA events) of K
+            steps, max over ranks, L2 flushed between steps outside the timed
+            intervals;
+  e2e       the same metric through the reference-facing C-ABI calls with host
+            buffers: per step upload of U from pinned host memory, CFL step,
+            RK3 step, download of U (eb2_upload / eb2_delta_t / eb2_rk_step /
+            eb2_download);
+  roofline  algorithmic HBM bytes of the fused stage kernel (256 B per cell per
+            RK3 step: 64 + 96 + 96) over its measured device time, against the
+            measured copy bandwidth;
+  cpu_baseline  the reference built from its own sources (oracle/_ref), all
+            host cores, on a bounded sample of the same workload.
+With --impl reference, rank 0 times the reference's CPU implementation on the
+same workload and prints the reference line; other ranks exit.
+For N > 1 (torchrun) every rank runs an independent replica (weak scaling):
+a single solve of this size does not shard in this build.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 1024
+ORDER, SCHEME = 3, 2          # SSP-RK3, HLLC
+BYTES_PER_CELL_STEP = 256     # 64 + 96 + 96 algorithmic HBM bytes (FP64 state)
+FLUSH_BYTES = 256 << 20       # > 126 MB L2
+METRIC = "cell-updates/s"
+WORKLOAD = "four-quadrant Riemann 1024x1024, characteristic WENO5-JS + HLLC + SSP-RK3, FP64"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(extra=None):
+    c = {"workload": WORKLOAD, "nx": NX, "ny": NY, "order": ORDER, "scheme": "HLLC",
+         "reconstruction": "WENO5-JS characteristic", "cfl": 0.5, "dtype": "f64",
+         "l2": "flushed between timed steps (256 MiB write outside the timed intervals)",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu_index)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------------------- dist
+def dist_setup(n, collective=True):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and collective:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def physical_gpu(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v for v in vis.split(",") if v.strip()]
+        if local < len(ids) and ids[local].strip().isdigit():
+            return int(ids[local])
+    return local
+
+
+# --------------------------------------------------------------------------- CPU
+def reference_lib():
+    """The reference built from its own sources, else the oracle port."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+    from oracle.bind import Oracle, Reference
+    if Reference.available("wjs"):
+        return Reference("wjs"), "reference"
+    return Oracle(), "port"
+
+
+def cpu_rate(budget_s: float, max_steps: int, warmup: int):
+    """Cell-updates/s of the CPU implementation on the benchmark workload:
+    full 1024^2 RK3 steps until the time budget is spent."""
+    from oracle.bind import FOUR_QUADRANT, Oracle
+    lib, kind = reference_lib()
+    orc = Oracle()
+    p = orc.params(NX, NY, recon=5, characteristic=1, weno_z=0, cfl=0.5)
+    U, lx, ly, _ = orc.init_case(p, FOUR_QUADRANT)
+    dx, dy = lx / NX, ly / NY
+    for _ in range(warmup):
+        lib.rk(p, ORDER, SCHEME, U, lib.dt(p, U, dx, dy), dx, dy)
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        dt = lib.dt(p, U, dx, dy)
+        lib.rk(p, ORDER, SCHEME, U, dt, dx, dy)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return NX * NY * n / el, el / n, n, kind, cores
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    # bounded: at most ~150 s of timed CPU work whatever K is
+    rate, per_step, n, kind, cores = cpu_rate(150.0, args.steps, min(args.warmup, 1))
+    line = {
+        "metric": METRIC, "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
+        "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": per_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config(), "impl": "reference",
+        "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": kind,
+                         "sample": f"{n} full SSP-RK3 steps of the 1024^2 grid"},
+        "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- GPU
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import overheatingproblem_b200 as eb2
+
+    s = eb2.Solver(NX, NY, device=local, recon=5, characteristic=True, weno_z=False, cfl=0.5)
+    lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    dx, dy = lx / NX, ly / NY
+    # warm-up (kernel attributes, clocks)
+    s.bench_steps(ORDER, SCHEME, dx, dy, max(args.warmup, 3), 0)
+    s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    torch.cuda.synchronize(local)
+    sampler = ClockSampler(physical_gpu(local)) if rank == 0 else None
+    barrier(world)
+    torch.cuda.synchronize(local)
+    step_ms, stage_ms, nstage, launches = s.bench_steps(ORDER, SCHEME, dx, dy, args.steps,
+                                                        FLUSH_BYTES)
+    torch.cuda.synchronize(local)
+    barrier(world)
+    clocks = sampler.stop() if sampler else None
+    st = s.status()
+    total_ms = allreduce_max(float(sum(step_ms)), world)
+    value = world * NX * NY * args.steps / (total_ms * 1e-3)
+
+    # roofline of the fused stage kernel
+    peak, peak_kind = hbm_peak()
+    alg_bytes = NX * NY * BYTES_PER_CELL_STEP * args.steps
+    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "eb2::fp64stage::k_stage (fused x+y sweep + RK stage)",
+                "per_launch_ms": stage_ms / nstage, "peak_kind": peak_kind,
+                "alg_bytes_per_launch": NX * NY * BYTES_PER_CELL_STEP / ORDER}
+
+    # end to end through the C ABI with host buffers
+    s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    host = torch.empty((4, NX + 8, NY + 8), dtype=torch.float64, pin_memory=True).numpy()
+    s.download(host)
+    k_e2e = max(3, min(args.steps, 50))
+    for _ in range(2):
+        s.upload(host)
+        dt = s.delta_t(dx, dy)
+        s.rk_step(ORDER, SCHEME, dt, dx, dy)
+        s.download(host)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        s.upload(host)
+        dt = s.delta_t(dx, dy)
+        s.rk_step(ORDER, SCHEME, dt, dx, dy)
+        s.download(host)
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": world * NX * NY * k_e2e / e2e_s, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes) + 8,
+           "steps": k_e2e, "path": "eb2_upload + eb2_delta_t + eb2_rk_step + eb2_download"}
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, per_step, n, kind, cores = cpu_rate(20.0, 40, 1)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": kind,
+               "sample": f"{n} full SSP-RK3 steps of the 1024^2 grid ({per_step:.3f} s each)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches, "status_flags": st,
+            "step_ms_min_median_max": [min(step_ms), float(np.median(step_ms)), max(step_ms)],
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    # the reference arm uses no collective: rank 0 works, the others leave
+    world, rank, local = dist_setup(args.gpus, collective=args.impl == "ours")
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,241 @@
+/*
+ * euler_b200.h -- C ABI of libeuler_b200.so, the B200 (sm_100a) 2D Euler
+ * finite-volume step.
+ *
+ * The entry points replace the operator API of the reference solver
+ * (xujf520/OverheatingProblem): the static inline C functions of its headers
+ * that src/RP_FVM.c calls, plus the control file reader.  Each declaration
+ * cites the reference function it stands in for.  Plain pointers and sizes
+ * only; no CUDA or C++ types cross this boundary.
+ *
+ * Model.  A context (eb2_ctx) owns one solve: its conserved state
+ * double U[4][nx+8][ny+8] (the reference's layout: x index i = row, y index j
+ * = unit stride, 4 ghost layers) lives in GPU memory, together with every
+ * temporary the step needs, allocated once at creation.  The reference's
+ * mutable globals (M_gamma, CFL, Recon_Accur, Characteriz, Source, Gravity,
+ * bc_config) become per-context settings.  Calls on one context are ordered
+ * on its CUDA stream and return after the result is complete; contexts are
+ * independent of one another.
+ *
+ * Arrays passed by the host are full [4][rows][cols] (or [4][4][rows][cols])
+ * double arrays in host memory, rows = nx + 8, cols = ny + 8.
+ *
+ * Return values: EB2_OK (0) or one of the EB2_E* codes; eb2_last_error()
+ * gives the message of the calling thread's last failure.
+ */
+#ifndef EULER_B200_H
+#define EULER_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct eb2_ctx eb2_ctx;
+
+enum {
+    EB2_OK = 0,
+    EB2_EARG = 1,         /* invalid argument                                     */
+    EB2_ENOMEM = 2,       /* device or host allocation failed                     */
+    EB2_ECUDA = 3,        /* CUDA error, or no CUDA device (there is no CPU path) */
+    EB2_ENONPHYS = 4,     /* non-physical state met (see eb2_status)              */
+    EB2_EUNSUPPORTED = 5  /* option the library does not implement               */
+};
+
+/* Status bits accumulated by the kernels of a context. */
+enum {
+    EB2_ST_NONPHYSICAL = 1, /* reconstructed rho<=0, p<=0 or NaN at an interface  */
+    EB2_ST_NAN_STATE = 2,   /* NaN in an updated conserved state                  */
+    EB2_ST_BAD_DT = 4       /* non-finite or non-positive CFL time step            */
+};
+
+/* Boundary kinds: BC_Type, include/Boundary_Condition.h:21-27. */
+enum { EB2_BC_OUTFLOW = 0, EB2_BC_REFLECTION = 1, EB2_BC_PERIODICITY = 2,
+       EB2_BC_INFLOW = 3, EB2_BC_FIXED_VALUE = 4 };
+
+/* Arithmetic of the step. */
+enum { EB2_FP64 = 0,      /* plain drop-in: bit-identical to the reference        */
+       EB2_MIXED = 1 };   /* FP32 reconstruction/fluxes, FP64 state and RK sums   */
+
+/* Initial states for eb2_init_case: the reference's TestCase2D values
+ * (include/Golbal.h:8-30) that the library implements, plus two cases that
+ * take their parameters from `q`. */
+enum {
+    EB2_CASE_PRECISION = 0,          /* TEST_PRECISION                           */
+    EB2_CASE_SOD_1D = 1,             /* TEST_1D_SHOCKTUBE                        */
+    EB2_CASE_IMPACT_WALL_1D = 4,     /* TEST_1D_IMPACTWALL                       */
+    EB2_CASE_NOH_1D = 6,             /* TEST_1D_NOHPROBLEM                       */
+    EB2_CASE_RIEMANN_1 = 7,          /* TEST_2D_SHOCKTUBE_CASE1 .. CASE5 = 7..11 */
+    EB2_CASE_DOUBLE_MACH = 16,       /* TEST_DOUBLE_MACH_REFLECTION              */
+    EB2_CASE_FOUR_QUADRANT = 100,    /* q[16] = (rho,u,v,p) of the upper-right,
+                                        upper-left, lower-left, lower-right
+                                        quadrants of [0,1]^2; q == NULL gives
+                                        the 1.5/0.5323/0.138/0.5323 states     */
+    EB2_CASE_WALL_HEATING = 101      /* [0,1]x[0,0.02], rho=1, u=-q[0] (q==NULL:
+                                        q[0]=1), v=0, p=1e-4, reflecting x=0,
+                                        outflow x=1, periodic in y, t=0.6      */
+};
+
+/* --- context --------------------------------------------------------------- */
+
+/* One solve of nx x ny interior cells on CUDA device `device`.  Allocates all
+ * device memory the step needs.  Fails with EB2_ECUDA when no GPU is usable. */
+int eb2_ctx_create(eb2_ctx **out, int nx, int ny, int device);
+int eb2_ctx_destroy(eb2_ctx *ctx);
+
+/* Use a caller-owned cudaStream_t (passed as void*); NULL restores the
+ * context's own stream. */
+int eb2_set_stream(eb2_ctx *ctx, void *cuda_stream);
+
+/* set_material_parameters (src/RP_FVM.c:600-605): M_gamma, Source, Gravity, CFL. */
+int eb2_set_material(eb2_ctx *ctx, double gamma, int source, double gravity, double cfl);
+
+/* Recon_Accur and Characteriz (include/Golbal.h:58-60): recon 1 (first
+ * order), 2 (TVD: minmod on conserved, van Leer on characteristic variables)
+ * or 5 (WENO5).  weno_z selects the WENO-Z weights the reference's
+ * characteristic branch uses (include/Reconstruction.h:941-942); 0 gives
+ * Jiang-Shu weights there.  The component branch always uses Jiang-Shu. */
+int eb2_set_reconstruction(eb2_ctx *ctx, int recon, int characteristic, int weno_z);
+
+/* EB2_FP64 or EB2_MIXED. */
+int eb2_set_precision(eb2_ctx *ctx, int precision);
+
+/* Opt-in, not in the reference: at an interface whose reconstructed states
+ * have rho<=0 or p<=0, use the two adjacent cell averages instead. */
+int eb2_set_positivity_fallback(eb2_ctx *ctx, int on);
+
+/* bc_config (include/Boundary_Condition.h:30-38). */
+int eb2_set_bc(eb2_ctx *ctx, int left, int right, int bottom, int top);
+/* inflow_state (Boundary_Condition.h:41,49) and L/R/B/T_fixed_value_state
+ * (include/initialize.h:1298-1301), conserved variables; NULL keeps a value. */
+int eb2_set_bc_states(eb2_ctx *ctx, const double *inflow4, const double *fixed16);
+/* Use BC_DoubleMach_2D (Boundary_Condition.h:480-692) for all four sides. */
+int eb2_set_double_mach(eb2_ctx *ctx, int on);
+
+/* --- state ------------------------------------------------------------------- */
+
+/* Init_Euler_2D (include/initialize.h:1558-1606): writes the initial conserved
+ * state of case `test_case` on the device, sets the case's boundary kinds and
+ * returns its domain lengths and final time. */
+int eb2_init_case(eb2_ctx *ctx, int test_case, const double *q, double *lx, double *ly,
+                  double *tmax);
+
+/* Copy the full state (ghosts included) between host and device. */
+int eb2_upload(eb2_ctx *ctx, const double *U);
+int eb2_download(eb2_ctx *ctx, double *U);
+
+/* Device address of the state, for callers that manage device memory. */
+int eb2_state_device_ptr(eb2_ctx *ctx, double **dptr);
+
+/* --- operators (each replaces the reference function named) --------------- */
+
+/* Boundary_Conditions (include/Boundary_Condition.h:963-980) on the state;
+ * `time` is read only by the double-Mach boundary. */
+int eb2_bc_apply(eb2_ctx *ctx, double time);
+
+/* Con_to_Pri_2D (include/initialize.h:1437-1454): primitives of the state on
+ * the box [3, rows-4]^2 into pri[4][rows][cols]. */
+int eb2_con_to_pri(eb2_ctx *ctx, double *pri);
+
+/* Compute_Eigen_2DX / _2DY (include/Characteriz.h:300-500): from pri
+ * [4][rows][cols] into eig_l[4][4][rows][cols] (eig_l[k][m]: row k of L) and
+ * eig_r[4][4][rows][cols] (eig_r[m][k]). */
+int eb2_eigen(eb2_ctx *ctx, int dir, const double *pri, double *eig_l, double *eig_r);
+
+/* WENO5_Reconstruction / TVD_Reconstruction / Reconstruction_Godunov
+ * (include/Reconstruction.h:887, 260, 51) of the state along dir (1 = x,
+ * 2 = y) into conserl / conserr [4][rows][cols]. */
+int eb2_reconstruct(eb2_ctx *ctx, int dir, double dx, double dy, double *conserl,
+                    double *conserr);
+
+/* HLL_Flux / HLLC_Flux / Roe_Flux / LLF_Flux (include/scheme.h:400, 690, 1018,
+ * 229) for AR_scheme `scheme` along dir; entries the reference's HLL skips are
+ * left as they were in `flux`. */
+int eb2_riemann(eb2_ctx *ctx, int scheme, int dir, const double *conserl,
+                const double *conserr, double *flux);
+
+/* Flux_Reconstruction_RP (include/CFD_convection.h:38-200) of the state. */
+int eb2_flux_reconstruction(eb2_ctx *ctx, int scheme, double dx, double dy, double *f,
+                            double *g);
+
+/* Space_Discrete_Item (include/scheme.h:3758-3777) with the gravity source of
+ * the state (Source_Gravity, :3723) when Source is on. */
+int eb2_space_discrete(eb2_ctx *ctx, double dx, double dy, const double *f, const double *g,
+                       double *L);
+
+/* Get_Delta_T_2D (include/function.h:144-175). */
+int eb2_delta_t(eb2_ctx *ctx, double dx, double dy, double *dt);
+/* The two maxima it combines: max(|u|+a), max(|v|+a) over the interior. */
+int eb2_wave_speeds(eb2_ctx *ctx, double *sx, double *sy);
+
+/* RK1_TimeAd / RK2_TimeAd / RK3_TimeAd (include/time_advance.h:643, 711, 788):
+ * one step of `order` with Riemann solver `scheme`; `time` is read only by
+ * the double-Mach boundary.  Returns EB2_ENONPHYS when a kernel met a
+ * non-physical state (the step still completes, as the reference's does). */
+int eb2_rk_step(eb2_ctx *ctx, int order, int scheme, double dt, double dx, double dy,
+                double time);
+
+/* The time loop of src/RP_FVM.c:179-267 (Control_Compution = 0) run on the
+ * device: CFL time step, clipping at the n_out output times and at tmax,
+ * `order`-stage SSP-RK steps.  Steps are issued in CUDA graphs of a few steps
+ * without host round trips.  At each output time the loop pauses and calls
+ * on_output(user, time, step) (may be NULL), from which the caller may read
+ * the state.  Returns the step count and the final time. */
+typedef void (*eb2_output_fn)(void *user, double time, long long step);
+int eb2_run(eb2_ctx *ctx, int order, int scheme, double dx, double dy, double t0,
+            double tmax, int n_out, eb2_output_fn on_output, void *user, long long *steps,
+            double *t_final);
+
+/* No reference counterpart: advance exactly `nsteps` steps of the device time
+ * loop (CFL time step from the device reduction, no output or tmax clipping),
+ * issued as CUDA graphs.  Used for fixed-length runs and benchmarks. */
+int eb2_advance(eb2_ctx *ctx, int order, int scheme, double dx, double dy, int nsteps);
+
+/* No reference counterpart: benchmark helper.  Runs `nsteps` steps as
+ * eb2_advance does, but launched one by one with CUDA events around each step
+ * and around each stage kernel, and a write of `flush_bytes` bytes between
+ * steps (outside the timed intervals) to evict the L2 cache.  step_ms[s]
+ * receives the device time of step s; *stage_ms the summed device time of the
+ * fused stage kernels and *stage_launches their count; *launches the number of
+ * library kernels launched inside the timed intervals. */
+int eb2_bench_steps(eb2_ctx *ctx, int order, int scheme, double dx, double dy, int nsteps,
+                    unsigned long long flush_bytes, float *step_ms, float *stage_ms,
+                    int *stage_launches, long long *launches);
+
+/* --- diagnostics ------------------------------------------------------------- */
+
+int eb2_status(eb2_ctx *ctx, unsigned *flags);
+int eb2_clear_status(eb2_ctx *ctx);
+int eb2_synchronize(eb2_ctx *ctx);
+const char *eb2_last_error(void);
+const char *eb2_version(void);
+
+/* --- control file -------------------------------------------------------------- */
+
+/* ControlParams (src/RP_FVM.c:66-82). */
+typedef struct {
+    int test_case;
+    int L_nx, L_ny;
+    int Time_ADM;
+    int scheme;
+    double M_gamma;
+    int Source;
+    double Gravity;
+    double CFL;
+    double Tmax;
+    int Control_Compution;
+    int Control_output;
+    int Recon_Accur;
+    int Characteriz;
+    char output_dir[256];
+} eb2_control;
+
+/* ReadControlFile (src/RP_FVM.c:382-589): the reference's defaults, then the
+ * `key: value` lines of the file ('#' comments), with its test-case names and
+ * its warnings on stderr.  Returns EB2_EARG when the file cannot be opened
+ * (the reference exits instead). */
+int eb2_read_control_file(const char *path, eb2_control *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EULER_B200_H */

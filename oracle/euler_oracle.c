@@ -821,7 +821,7 @@ int orc_init_case(orc_params *p, int which, const double *q, double *U,
     const size_t n = (size_t)4 * rows * cols;
     double *W = (double *)calloc(n, sizeof(double));
     if (!W) return -2;
-    p->dmr = 0;
+    p->dmr = 0;  /* only the double-Mach case's caller turns the exact boundary on */
     switch (which) {
         case ORC_CASE_FOUR_QUADRANT: {
             /* states ordered upper-right, upper-left, lower-left, lower-right */
@@ -854,8 +854,11 @@ int orc_init_case(orc_params *p, int which, const double *q, double *U,
             /* initEulerpri2D_DoubleMachReflection, include/initialize.h:890-952 */
             const double post[4] = {8.0, 7.1447, -4.125, 116.5}, pre[4] = {1.4, 0.0, 0.0, 1.0};
             const double slope = sqrt(3.0), x0 = 1.0 / 6.0;
+            /* the case's own boundary kinds (:900-903); the exact double-Mach
+               boundary is selected separately by setting p->dmr */
+            p->bc[0] = ORC_BC_INFLOW; p->bc[1] = ORC_BC_OUTFLOW;
+            p->bc[2] = ORC_BC_REFLECT; p->bc[3] = ORC_BC_REFLECT;
             *lx = 4.0; *ly = 1.0; *tmax = 0.2;
-            p->dmr = 1;
             double nxd = rows - 2 * gc, nyd = cols - 2 * gc;
             for (int i = gc; i < rows - gc; i++)
                 for (int j = gc; j < cols - gc; j++) {

@@ -1,0 +1,423 @@
+// eb2_point_fp64.cuh -- per-interface FP64 arithmetic of the plain drop-in.
+//
+// Every expression keeps the reference's evaluation order and the translation
+// units that include this header are compiled with -fmad=false, so each
+// function returns the same bits as the reference's C code built with gcc -O3
+// (which contracts nothing into FMAs on x86-64 without -march).  Reference
+// locations are cited per function.
+#pragma once
+
+#include "eb2_common.cuh"
+
+namespace eb2 {
+namespace x64 {
+
+// Roe-averaged quantities at an interface between cells a and b
+// (include/Characteriz.h:333-342 and :435-444).
+struct Roe {
+    double u, v, H, c, q2, b1, b2, ic, uc, vc;  // ic = 1/c, uc = u/c, vc = v/c
+};
+
+// a = (rho, u, v, p, H) of the left cell, b of the right cell.
+__device__ __forceinline__ Roe roe_average(const double* a, const double* b, double gm1) {
+    Roe r;
+    double D = sqrt(b[0] / a[0]);
+    double D1 = D + 1.0;
+    r.u = (a[1] + D * b[1]) / D1;
+    r.v = (a[2] + D * b[2]) / D1;
+    r.H = (a[4] + D * b[4]) / D1;
+    r.q2 = r.u * r.u + r.v * r.v;
+    double c2 = gm1 * (r.H - 0.5 * r.q2);
+    r.c = sqrt(c2);
+    r.b1 = gm1 / c2;
+    r.b2 = 1.0 + r.b1 * r.q2 - r.b1 * r.H;
+    r.ic = 1.0 / r.c;
+    r.uc = r.u / r.c;
+    r.vc = r.v / r.c;
+    return r;
+}
+
+// Row k of the left-eigenvector matrix (eigen_l[k][*], Characteriz.h:346-367
+// for x, :448-469 for y).
+template <int DIR>
+__device__ __forceinline__ void left_row(const Roe& e, int k, double* l) {
+    if (DIR == 1) {
+        switch (k) {
+            case 0: l[0] = 0.5 * (e.b2 + e.uc); l[1] = -0.5 * (e.b1 * e.u + e.ic);
+                    l[2] = -0.5 * e.b1 * e.v; l[3] = 0.5 * e.b1; break;
+            case 1: l[0] = -e.q2 + e.H; l[1] = e.u; l[2] = e.v; l[3] = -1.0; break;
+            case 2: l[0] = e.v; l[1] = 0.0; l[2] = -1.0; l[3] = 0.0; break;
+            default: l[0] = 0.5 * (e.b2 - e.uc); l[1] = 0.5 * (-e.b1 * e.u + e.ic);
+                     l[2] = 0.5 * -e.b1 * e.v; l[3] = 0.5 * e.b1; break;
+        }
+    } else {
+        switch (k) {
+            case 0: l[0] = 0.5 * (e.b2 + e.vc); l[1] = -0.5 * (e.b1 * e.u + 0.0 / e.c);
+                    l[2] = -0.5 * (e.b1 * e.v + e.ic); l[3] = 0.5 * e.b1; break;
+            case 1: l[0] = -e.q2 + e.H; l[1] = e.u; l[2] = e.v; l[3] = -1.0; break;
+            case 2: l[0] = -e.u; l[1] = 1.0; l[2] = -0.0; l[3] = 0.0; break;
+            default: l[0] = 0.5 * (e.b2 - e.vc); l[1] = 0.5 * (-e.b1 * e.u + 0.0 / e.c);
+                     l[2] = 0.5 * (-e.b1 * e.v + e.ic); l[3] = 0.5 * e.b1; break;
+        }
+    }
+}
+
+// Row m of the right-eigenvector matrix, R[m][k] = eigen_r[m][k]
+// (Characteriz.h:371-392 for x, :473-494 for y).
+template <int DIR>
+__device__ __forceinline__ void right_row(const Roe& e, int m, double* r) {
+    if (DIR == 1) {
+        switch (m) {
+            case 0: r[0] = 1.0; r[1] = e.b1; r[2] = 0.0; r[3] = 1.0; break;
+            case 1: r[0] = e.u - 1.0 * e.c; r[1] = e.u * e.b1; r[2] = 0.0; r[3] = e.u + 1.0 * e.c; break;
+            case 2: r[0] = e.v - 0.0 * e.c; r[1] = e.v * e.b1; r[2] = -1.0; r[3] = e.v + 0.0 * e.c; break;
+            default: r[0] = e.H - e.u * e.c; r[1] = e.H * e.b1 - 1.0; r[2] = -e.v; r[3] = e.H + e.u * e.c; break;
+        }
+    } else {
+        switch (m) {
+            case 0: r[0] = 1.0; r[1] = e.b1; r[2] = 0.0; r[3] = 1.0; break;
+            case 1: r[0] = e.u - 0.0 * e.c; r[1] = e.u * e.b1; r[2] = 1.0; r[3] = e.u + 0.0 * e.c; break;
+            case 2: r[0] = e.v - 1.0 * e.c; r[1] = e.v * e.b1; r[2] = -0.0; r[3] = e.v + 1.0 * e.c; break;
+            default: r[0] = e.H - e.v * e.c; r[1] = e.H * e.b1 - 1.0; r[2] = e.u; r[3] = e.H + e.v * e.c; break;
+        }
+    }
+}
+
+// Jiang-Shu smoothness indicators (include/Reconstruction.h:1425-1432).
+__device__ __forceinline__ void smooth3(double v1, double v2, double v3, double v4, double v5,
+                                        double& s1, double& s2, double& s3) {
+    s1 = 13.0 / 12.0 * (v1 - 2.0 * v2 + v3) * (v1 - 2.0 * v2 + v3)
+       + 0.25 * (v1 - 4.0 * v2 + 3.0 * v3) * (v1 - 4.0 * v2 + 3.0 * v3);
+    s2 = 13.0 / 12.0 * (v2 - 2.0 * v3 + v4) * (v2 - 2.0 * v3 + v4)
+       + 0.25 * (v2 - v4) * (v2 - v4);
+    s3 = 13.0 / 12.0 * (v3 - 2.0 * v4 + v5) * (v3 - 2.0 * v4 + v5)
+       + 0.25 * (3.0 * v3 - 4.0 * v4 + v5) * (3.0 * v3 - 4.0 * v4 + v5);
+}
+
+// Nonlinear blend of the three candidate stencils (Reconstruction.h:1440-1454).
+__device__ __forceinline__ double blend3(double a1, double a2, double a3, double v1, double v2,
+                                         double v3, double v4, double v5) {
+    double w1 = a1 / (a1 + a2 + a3);
+    double w2 = a2 / (a1 + a2 + a3);
+    double w3 = a3 / (a1 + a2 + a3);
+    return w1 * (2.0 * v1 - 7.0 * v2 + 11.0 * v3) / 6.0
+         + w2 * (-v2 + 5.0 * v3 + 2.0 * v4) / 6.0
+         + w3 * (2.0 * v3 + 5.0 * v4 - v5) / 6.0;
+}
+
+// WENO5_L with Jiang-Shu weights (Reconstruction.h:1408-1455); WENO5_R is the
+// same function on the mirrored stencil.
+__device__ __forceinline__ double weno5_js(double v1, double v2, double v3, double v4, double v5) {
+    const double eps = 1.0e-15;
+    double s1, s2, s3;
+    smooth3(v1, v2, v3, v4, v5, s1, s2, s3);
+    double a1 = 0.1 / (eps + s1) / (eps + s1);
+    double a2 = 0.6 / (eps + s2) / (eps + s2);
+    double a3 = 0.3 / (eps + s3) / (eps + s3);
+    return blend3(a1, a2, a3, v1, v2, v3, v4, v5);
+}
+
+// WENO5Z_L / WENO5Z_R (Reconstruction.h:1519-1624).
+__device__ __forceinline__ double weno5_z(double v1, double v2, double v3, double v4, double v5) {
+    const double eps = 1.0e-15;
+    double s1, s2, s3;
+    smooth3(v1, v2, v3, v4, v5, s1, s2, s3);
+    double tau = fabs(s1 - s3);
+    double a1 = 0.1 * (1.0 + tau / (s1 + eps));
+    double a2 = 0.6 * (1.0 + tau / (s2 + eps));
+    double a3 = 0.3 * (1.0 + tau / (s3 + eps));
+    return blend3(a1, a2, a3, v1, v2, v3, v4, v5);
+}
+
+__device__ __forceinline__ int sgn(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+
+// TVD_minmod_* / TVD_vanleer_* (Reconstruction.h:1088-1201) with the limiters
+// min_mod and van_leer of include/function.h:66-74.  side +1 returns the value
+// at the right face of cell c, side -1 at its left face.
+template <bool VANLEER>
+__device__ __forceinline__ double muscl(double lo, double c, double hi, double delta, int side) {
+    double s1 = (c - lo) / delta;
+    double s2 = (hi - c) / delta;
+    double s;
+    if (VANLEER) {
+        double tiny = 1.0e-6;
+        s = ((sgn(s1) + sgn(s2)) * s1 * s2) / (fabs(s1) + fabs(s2) + tiny);
+    } else {
+        double a = fabs(s1), b = fabs(s2);
+        s = 0.5 * (sgn(s1) + sgn(s2)) * (a > b ? b : a);
+    }
+    return side > 0 ? c + 0.5 * s * delta : c - 0.5 * s * delta;
+}
+
+// Interface pair (minus side, plus side) from six values q[0..5] = cells
+// i-2..i+3 of one field; RECON 5 = WENO5, 2 = TVD, 1 = first order.
+template <int RECON, bool WZ, bool VANLEER>
+__device__ __forceinline__ void recon_pair(const double* q, double delta, double& qm, double& qp) {
+    if (RECON == 5) {
+        if (WZ) {
+            qm = weno5_z(q[0], q[1], q[2], q[3], q[4]);
+            qp = weno5_z(q[5], q[4], q[3], q[2], q[1]);
+        } else {
+            qm = weno5_js(q[0], q[1], q[2], q[3], q[4]);
+            qp = weno5_js(q[5], q[4], q[3], q[2], q[1]);
+        }
+    } else if (RECON == 2) {
+        qm = muscl<VANLEER>(q[1], q[2], q[3], delta, +1);
+        qp = muscl<VANLEER>(q[2], q[3], q[4], delta, -1);
+    } else {
+        qm = q[2];
+        qp = q[3];
+    }
+}
+
+// Left/right states unpacked as the flux routines of include/scheme.h do.
+struct Side {
+    double r, ru, rv, re, ir, u, v, uu, vv, p;
+};
+
+__device__ __forceinline__ Side unpack(const double* q, double gm1) {
+    Side s;
+    s.r = q[0]; s.ru = q[1]; s.rv = q[2]; s.re = q[3];
+    s.ir = 1.0 / s.r;
+    s.u = s.ru * s.ir;
+    s.v = s.rv * s.ir;
+    s.uu = s.u * s.u;
+    s.vv = s.v * s.v;
+    s.p = (s.re - 0.5 * s.r * (s.uu + s.vv)) * gm1;
+    return s;
+}
+
+// Physical flux along DIR with total enthalpy H.
+template <int DIR>
+__device__ __forceinline__ void phys_flux(const Side& s, double H, double* F) {
+    if (DIR == 1) {
+        F[0] = s.r * s.u;
+        F[1] = s.r * s.uu + s.p;
+        F[2] = s.r * s.v * s.u;
+        F[3] = s.r * H * s.u;
+    } else {
+        F[0] = s.r * s.v;
+        F[1] = s.r * s.u * s.v;
+        F[2] = s.r * s.vv + s.p;
+        F[3] = s.r * H * s.v;
+    }
+}
+
+// HLLC_Flux (include/scheme.h:690-1001).  The x sweep takes the sound speed
+// from the enthalpy (:745-746), the y sweep from gamma*p/rho (:895-896).
+template <int DIR>
+__device__ __forceinline__ void flux_hllc(const double* ql, const double* qr, const Gas& g,
+                                          double* F) {
+    Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
+    double HL, HR, aL, aR;
+    if (DIR == 1) {
+        HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+        HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+        aL = sqrt((g.gamma - 1.0) * (HL - 0.5 * (L.uu + L.vv)));
+        aR = sqrt((g.gamma - 1.0) * (HR - 0.5 * (R.uu + R.vv)));
+    } else {
+        aL = sqrt(g.gamma * L.p * L.ir);
+        aR = sqrt(g.gamma * R.p * R.ir);
+        HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+        HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    }
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double unL = DIR == 1 ? L.u : L.v, unR = DIR == 1 ? R.u : R.v;
+    double sqL = sqrt(L.r), sqR = sqrt(R.r);
+    double ssum = sqL + sqR;
+    double isum = 1.0 / ssum;
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double eta = DIR == 1 ? 0.5 * sqL * sqR * isum * isum : 0.5 * sqL * sqR / (ssum * ssum);
+    double dun = unR - unL;
+    double dd = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun);
+    double nbar = DIR == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+        return;
+    }
+    if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+        return;
+    }
+    double denom = L.r * (sl - unL) - R.r * (sr - unR);
+    double ss = (R.p - L.p + L.r * unL * (sl - unL) - R.r * unR * (sr - unR)) / denom;
+    if (ss >= 0.0) {
+        double m = L.r * (sl - unL) / (sl - ss);
+        double e = L.re * L.ir + (ss - unL) * (ss + L.p / (L.r * (sl - unL)));
+        F[0] = FL[0] + sl * (m - L.r);
+        if (DIR == 1) {
+            F[1] = FL[1] + sl * (m * ss - L.ru);
+            F[2] = FL[2] + sl * (m * L.v - L.rv);
+        } else {
+            F[1] = FL[1] + sl * (m * L.u - L.ru);
+            F[2] = FL[2] + sl * (m * ss - L.rv);
+        }
+        F[3] = FL[3] + sl * (m * e - L.re);
+    } else {
+        double m = R.r * (sr - unR) / (sr - ss);
+        double e = R.re * R.ir + (ss - unR) * (ss + R.p / (R.r * (sr - unR)));
+        F[0] = FR[0] + sr * (m - R.r);
+        if (DIR == 1) {
+            F[1] = FR[1] + sr * (m * ss - R.ru);
+            F[2] = FR[2] + sr * (m * R.v - R.rv);
+        } else {
+            F[1] = FR[1] + sr * (m * R.u - R.ru);
+            F[2] = FR[2] + sr * (m * ss - R.rv);
+        }
+        F[3] = FR[3] + sr * (m * e - R.re);
+    }
+}
+
+// HLL_Flux (include/scheme.h:400-674).  Returns false where the reference
+// skips the interface (`continue` on rho<=0, NaN rho, or NaN wave speed,
+// :427-436 and :500-503) and leaves its flux entry untouched.
+template <int DIR>
+__device__ __forceinline__ bool flux_hll(const double* ql, const double* qr, const Gas& g,
+                                         double* F) {
+    if (ql[0] <= 0.0 || qr[0] <= 0.0) return false;
+    if (isnan(ql[0]) || isnan(qr[0])) return false;
+    Side L = unpack(ql, g.gamma - 1.0), R = unpack(qr, g.gamma - 1.0);
+    double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+    double HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    double aL = sqrt((g.gamma - 1.0) * (HL - 0.5 * (L.uu + L.vv)));
+    double aR = sqrt((g.gamma - 1.0) * (HR - 0.5 * (R.uu + R.vv)));
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double sqL = sqrt(L.r), sqR = sqrt(R.r);
+    double ssum = sqL + sqR;
+    double isum = 1.0 / ssum;
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double eta = 0.5 * sqL * sqR / (ssum * ssum);
+    double dun = DIR == 1 ? R.u - L.u : R.v - L.v;
+    double dd = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun);
+    if (isnan(dd)) return false;
+    double nbar = DIR == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    } else {
+        double idiff = 1.0 / (sr - sl);
+        double slsr = sl * sr;
+        const double UL[4] = {L.r, L.ru, L.rv, L.re}, UR[4] = {R.r, R.ru, R.rv, R.re};
+        for (int k = 0; k < 4; k++)
+            F[k] = (sr * FL[k] - sl * FR[k] + slsr * (UR[k] - UL[k])) * idiff;
+    }
+    return true;
+}
+
+// Roe_Flux (include/scheme.h:1018-1322); its entropy fix is a no-op
+// (:1117-1126), so |lambda| is used directly.
+template <int DIR>
+__device__ __forceinline__ void flux_roe(const double* ql, const double* qr, const Gas& g,
+                                         double* F) {
+    Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
+    double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+    double HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double sqL = sqrt(L.r), sqR = sqrt(R.r);
+    double isum = 1.0 / (sqL + sqR);
+    double rbar = sqL * sqR;
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double Hbar = (sqL * HL + sqR * HR) * isum;
+    double q2 = ubar * ubar + vbar * vbar;
+    double cbar = sqrt(g.gm1 * (Hbar - 0.5 * q2));
+    double nbar = DIR == 1 ? ubar : vbar;
+    double lam[4] = {fabs(nbar - cbar), fabs(nbar), fabs(nbar), fabs(nbar + cbar)};
+    double drho = R.r - L.r, du = R.u - L.u, dv = R.v - L.v, dp = R.p - L.p;
+    double c2 = cbar * cbar;
+    double i2c2 = 1.0 / (2.0 * c2);
+    double ic2 = 1.0 / c2;
+    double dn = DIR == 1 ? du : dv, dtn = DIR == 1 ? dv : du;
+    double al[4];
+    al[0] = (dp - rbar * cbar * dn) * i2c2;
+    al[1] = drho - dp * ic2;
+    al[2] = rbar * dtn;
+    al[3] = (dp + rbar * cbar * dn) * i2c2;
+    double K[4][4];
+    if (DIR == 1) {
+        K[0][0] = 1.0; K[0][1] = ubar - cbar; K[0][2] = vbar; K[0][3] = Hbar - ubar * cbar;
+        K[1][0] = 1.0; K[1][1] = ubar;        K[1][2] = vbar; K[1][3] = 0.5 * q2;
+        K[2][0] = 0.0; K[2][1] = 0.0;         K[2][2] = 1.0;  K[2][3] = vbar;
+        K[3][0] = 1.0; K[3][1] = ubar + cbar; K[3][2] = vbar; K[3][3] = Hbar + ubar * cbar;
+    } else {
+        K[0][0] = 1.0; K[0][1] = ubar; K[0][2] = vbar - cbar; K[0][3] = Hbar - vbar * cbar;
+        K[1][0] = 1.0; K[1][1] = ubar; K[1][2] = vbar;        K[1][3] = 0.5 * q2;
+        K[2][0] = 0.0; K[2][1] = 1.0;  K[2][2] = 0.0;         K[2][3] = ubar;
+        K[3][0] = 1.0; K[3][1] = ubar; K[3][2] = vbar + cbar; K[3][3] = Hbar + vbar * cbar;
+    }
+    for (int c = 0; c < 4; c++) F[c] = 0.5 * (FL[c] + FR[c]);
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        double term = 0.5 * lam[w] * al[w];
+#pragma unroll
+        for (int c = 0; c < 4; c++) F[c] -= term * K[w][c];
+    }
+}
+
+// LLF_Flux (include/scheme.h:229-381), the dispatch default.
+template <int DIR>
+__device__ __forceinline__ void flux_llf(const double* ql, const double* qr, const Gas& g,
+                                         double* F) {
+    Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
+    double aL = sqrt(g.gamma * L.p * L.ir), aR = sqrt(g.gamma * R.p * R.ir);
+    double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+    double HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double unL = DIR == 1 ? L.u : L.v, unR = DIR == 1 ? R.u : R.v;
+    double a = fabs(unL) + aL, b = fabs(unR) + aR;
+    double sp = a > b ? a : b;
+    const double UL[4] = {L.r, L.ru, L.rv, L.re}, UR[4] = {R.r, R.ru, R.rv, R.re};
+#pragma unroll
+    for (int k = 0; k < 4; k++) F[k] = 0.5 * (FL[k] + FR[k]) - 0.5 * sp * (UR[k] - UL[k]);
+}
+
+// Riemann dispatch.  Returns false when HLL skipped the interface.
+template <int FLUX, int DIR>
+__device__ __forceinline__ bool riemann(const double* ql, const double* qr, const Gas& g,
+                                        double* F) {
+    if (FLUX == FLUX_HLL) return flux_hll<DIR>(ql, qr, g, F);
+    if (FLUX == FLUX_HLLC) flux_hllc<DIR>(ql, qr, g, F);
+    else if (FLUX == FLUX_ROE) flux_roe<DIR>(ql, qr, g, F);
+    else flux_llf<DIR>(ql, qr, g, F);
+    return true;
+}
+
+// Primitive state of one cell plus its enthalpy: Con_to_Pri_2D
+// (include/initialize.h:1443-1446) and the H of Compute_Eigen_2DX
+// (include/Characteriz.h:319).
+__device__ __forceinline__ void primitive5(double r, double ru, double rv, double re,
+                                           const Gas& g, double* w) {
+    double u = ru / r;
+    double v = rv / r;
+    double p = (re - 0.5 * r * (u * u + v * v)) * g.gm1;
+    w[0] = r;
+    w[1] = u;
+    w[2] = v;
+    w[3] = p;
+    w[4] = 0.5 * (u * u + v * v) + g.gr * (p / r);
+}
+
+// Is a reconstructed conserved state admissible (rho > 0, p > 0, finite)?
+__device__ __forceinline__ bool admissible(const double* q, double gm1) {
+    double r = q[0];
+    if (!(r > 0.0)) return false;
+    double u = q[1] / r, v = q[2] / r;
+    double p = (q[3] - 0.5 * r * (u * u + v * v)) * gm1;
+    return p > 0.0;
+}
+
+}  // namespace x64
+}  // namespace eb2

@@ -1,0 +1,305 @@
+// eb2_stage_fp64.cuh -- fused x+y sweep and SSP-RK stage, FP64 bit-parity form.
+//
+// One CTA owns a TX x TY tile of cells (x rows i, y columns j).  It stages the
+// stage input of the tile plus a 3-cell halo in shared memory, converts the
+// tile and its first ring to primitives (Con_to_Pri_2D), computes every x and
+// y interface flux the tile needs (Roe eigenvectors, projection, WENO5/TVD
+// per field, back-projection, Riemann flux: WENO5_Reconstruction /
+// TVD_Reconstruction + HLLC_Flux etc. of Flux_Reconstruction_RP,
+// include/CFD_convection.h:38-200), and then forms the flux difference
+// (Space_Discrete_Item, include/scheme.h:3758-3777) and the SSP-RK combination
+// (include/time_advance.h:831-872) for its cells.  The stage output leaves
+// through one coalesced store per field; the state at the start of the step
+// is read once for stages 2 and 3.  The reference makes about twelve
+// full-grid passes with temporaries for the same stage.
+//
+// Wave-speed maxima of the new state (Get_Delta_T_2D's reduction,
+// include/function.h:144-175) are reduced per block in the epilogue.
+#pragma once
+
+#include "eb2_kernels.h"
+#include "eb2_point_fp64.cuh"
+
+namespace eb2 {
+namespace fp64stage {
+
+constexpr int TX = 16, TY = 32, NT = 256;
+constexpr int HX = TX + 6, HY = TY + 6;       // U tile with halos
+constexpr int PX = TX + 2, PY = TY + 2;       // primitive region (tile + first ring)
+constexpr int FS = HX * HY;                   // field stride in sU
+constexpr int PS = PX * PY;                   // field stride in sP
+constexpr int XS = (TX + 1) * TY;             // field stride in sFx
+constexpr int YS = TX * (TY + 1);             // field stride in sFy
+constexpr int NJX = (TX + 1) * TY, NJY = TX * (TY + 1);
+
+template <bool CHAR>
+constexpr size_t smem_bytes() {
+    return (size_t)(4 * FS + (CHAR ? 5 * PS : 0) + 4 * XS + 4 * YS) * sizeof(double);
+}
+
+// rho > 0 and p > 0 without a division: 2*rho*E > (rho u)^2 + (rho v)^2.
+__device__ __forceinline__ bool admissible(const double* q) {
+    return q[0] > 0.0 && 2.0 * q[3] * q[0] > q[1] * q[1] + q[2] * q[2];
+}
+
+// Flux at one interface.  s points at stencil cell n=0 (i-2) of field 0,
+// `stride` steps along the sweep, fields are FS apart.  pa/pb point at the
+// primitive 5-tuples of the two cells next to the interface (fields PS apart).
+template <int DIR, int RECON, bool CHAR, bool WZ, int FLUX>
+__device__ __forceinline__ unsigned interface_flux(const double* __restrict__ s, int stride,
+                                                   const double* __restrict__ pa,
+                                                   const double* __restrict__ pb, double delta,
+                                                   const Gas& g, int positivity,
+                                                   double* __restrict__ out, int ostride) {
+    constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 ? 1 : 2);
+    constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 ? 5 : 4);
+    double ql[4], qr[4];
+    if (CHAR) {
+        double A[5], B[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            A[q] = pa[q * PS];
+            B[q] = pb[q * PS];
+        }
+        const x64::Roe e = x64::roe_average(A, B, g.gm1);
+        double wm[4], wp[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double l[4];
+            x64::left_row<DIR>(e, k, l);
+            double q6[6];
+#pragma unroll
+            for (int n = N0; n < N1; n++) {
+                double acc = 0.0;
+#pragma unroll
+                for (int m = 0; m < 4; m++) acc += s[m * FS + n * stride] * l[m];
+                q6[n] = acc;
+            }
+            x64::recon_pair<RECON, WZ, true>(q6, delta, wm[k], wp[k]);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            double r[4];
+            x64::right_row<DIR>(e, m, r);
+            double sl = 0.0, sr = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                sl += wm[k] * r[k];
+                sr += wp[k] * r[k];
+            }
+            ql[m] = sl;
+            qr[m] = sr;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double q6[6];
+#pragma unroll
+            for (int n = N0; n < N1; n++) q6[n] = s[k * FS + n * stride];
+            x64::recon_pair<RECON, false, false>(q6, delta, ql[k], qr[k]);
+        }
+    }
+    unsigned st = 0;
+    if (!(admissible(ql) && admissible(qr))) {
+        if (positivity) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                ql[k] = s[k * FS + 2 * stride];
+                qr[k] = s[k * FS + 3 * stride];
+            }
+        } else {
+            st |= ST_NONPHYSICAL;
+        }
+    }
+    double F[4];
+    if (!x64::riemann<FLUX, DIR>(ql, qr, g, F)) {
+        // the reference leaves a stale entry here; a NaN makes it visible
+#pragma unroll
+        for (int k = 0; k < 4; k++) F[k] = __longlong_as_double(0x7ff8000000000000ll);
+        st |= ST_NONPHYSICAL;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k * ostride] = F[k];
+    return st;
+}
+
+template <int RECON, bool CHAR, bool WZ, int FLUX>
+__global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
+    Ctrl* ctrl = a.ctrl;
+    if (!ctrl->active) return;
+    extern __shared__ double sm[];
+    double* sU = sm;
+    double* sP = sU + 4 * FS;
+    double* sFx = sP + (CHAR ? 5 * PS : 0);
+    double* sFy = sFx + 4 * XS;
+    __shared__ double red[3][NT / 32];
+
+    const int rows = a.grid.rows, cols = a.grid.cols;
+    const int i0 = GC + blockIdx.y * TX, j0 = GC + blockIdx.x * TY;
+    const double* __restrict__ uin = a.uin;
+    const Gas g = a.gas;
+
+    // 1. stage input tile + halo (rows i0-3..i0+TX+2, columns j0-3..j0+TY+2)
+    for (int e = threadIdx.x; e < 4 * FS; e += NT) {
+        int k = e / FS, rem = e - k * FS;
+        int r = rem / HY, c = rem - r * HY;
+        int i = i0 - 3 + r, j = j0 - 3 + c;
+        sU[e] = (i < rows && j < cols) ? uin[at(k, i, j, rows, cols)] : 0.0;
+    }
+    __syncthreads();
+
+    // 2. primitives of the tile and its first ring
+    if (CHAR) {
+        for (int e = threadIdx.x; e < PS; e += NT) {
+            int r = e / PY, c = e - r * PY;
+            int u = (r + 2) * HY + (c + 2);
+            double w[5];
+            x64::primitive5(sU[u], sU[FS + u], sU[2 * FS + u], sU[3 * FS + u], g, w);
+#pragma unroll
+            for (int q = 0; q < 5; q++) sP[q * PS + e] = w[q];
+        }
+        __syncthreads();
+    }
+
+    // 3. interface fluxes: x faces (TX+1) x TY, then y faces TX x (TY+1)
+    unsigned st = 0;
+    const int pos = a.num.positivity;
+    for (int job = threadIdx.x; job < NJX + NJY; job += NT) {
+        if (job < NJX) {
+            int rr = job / TY, cc = job - rr * TY;
+            const double* s = sU + rr * HY + (cc + 3);
+            const double* pa = sP + rr * PY + (cc + 1);
+            st |= interface_flux<1, RECON, CHAR, WZ, FLUX>(s, HY, pa, pa + PY, a.grid.dx, g, pos,
+                                                           sFx + rr * TY + cc, XS);
+        } else {
+            int q = job - NJX;
+            int rr = q / (TY + 1), cc = q - rr * (TY + 1);
+            const double* s = sU + (rr + 3) * HY + cc;
+            const double* pa = sP + (rr + 1) * PY + cc;
+            st |= interface_flux<2, RECON, CHAR, WZ, FLUX>(s, 1, pa, pa + 1, a.grid.dy, g, pos,
+                                                           sFy + rr * (TY + 1) + cc, YS);
+        }
+    }
+    __syncthreads();
+
+    // 4. flux difference, source, RK combination, wave-speed partials
+    const double dt = ctrl->dt;
+    const double idx = a.grid.inv_dx, idy = a.grid.inv_dy;
+    const double grav = a.num.gravity;
+    double mx = 0.0, my = 0.0, ps = 0.0;
+    for (int e = threadIdx.x; e < TX * TY; e += NT) {
+        int rr = e / TY, cc = e - rr * TY;
+        int i = i0 + rr, j = j0 + cc;
+        if (i >= rows - GC || j >= cols - GC) continue;
+        int u = (rr + 3) * HY + (cc + 3);
+        double x[4], src[4] = {0.0, 0.0, 0.0, 0.0}, o[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) x[k] = sU[k * FS + u];
+        if (a.num.source) {
+            // Source_Gravity, include/scheme.h:3738-3749
+            double rho = x[0];
+            double v = x[2] / rho;
+            src[2] = rho * grav;
+            src[3] = rho * grav * v;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double fxp = sFx[k * XS + (rr + 1) * TY + cc], fxm = sFx[k * XS + rr * TY + cc];
+            double fyp = sFy[k * YS + rr * (TY + 1) + cc + 1], fym = sFy[k * YS + rr * (TY + 1) + cc];
+            double L = -(fxp - fxm) * idx - (fyp - fym) * idy + src[k];
+            double y = a.combine == COMB_EULER ? x[k] : a.un[at(k, i, j, rows, cols)];
+            double r;
+            switch (a.combine) {
+                case COMB_EULER: r = y + dt * L; break;
+                case COMB_RK2: r = 0.5 * y + 0.5 * (x[k] + dt * L); break;
+                case COMB_RK3_2: r = (3.0 / 4.0) * y + (1.0 / 4.0) * (x[k] + dt * L); break;
+                default: r = (1.0 / 3.0) * y + (2.0 / 3.0) * (x[k] + dt * L); break;
+            }
+            o[k] = r;
+            a.uout[at(k, i, j, rows, cols)] = r;
+        }
+        if (isnan(o[0]) || isnan(o[1]) || isnan(o[2]) || isnan(o[3])) st |= ST_NAN_STATE;
+        if (a.partials) {
+            double rho = o[0];
+            double uu = o[1] / rho, vv = o[2] / rho;
+            double p = (o[3] - 0.5 * rho * (uu * uu + vv * vv)) * g.gm1;
+            double c = sqrt(g.gamma * p / rho);
+            double lx = fabs(uu) + c, ly = fabs(vv) + c;
+            if (lx > mx) mx = lx;
+            if (ly > my) my = ly;
+            ps += p;
+        }
+    }
+
+    unsigned wst = __reduce_or_sync(0xffffffffu, st);
+    if (wst && (threadIdx.x & 31) == 0) atomicOr(&ctrl->status, wst);
+
+    if (a.partials) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            double ox = __shfl_down_sync(0xffffffffu, mx, off);
+            double oy = __shfl_down_sync(0xffffffffu, my, off);
+            double op = __shfl_down_sync(0xffffffffu, ps, off);
+            if (ox > mx) mx = ox;
+            if (oy > my) my = oy;
+            ps += op;
+        }
+        int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) {
+            red[0][w] = mx;
+            red[1][w] = my;
+            red[2][w] = ps;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bx = 0.0, by = 0.0, bp = 0.0;
+            for (int q = 0; q < NT / 32; q++) {
+                if (red[0][q] > bx) bx = red[0][q];
+                if (red[1][q] > by) by = red[1][q];
+                bp += red[2][q];
+            }
+            size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+            a.partials[3 * b + 0] = bx;
+            a.partials[3 * b + 1] = by;
+            a.partials[3 * b + 2] = bp;
+        }
+    }
+}
+
+template <int RECON, bool CHAR, bool WZ, int FLUX>
+cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
+    constexpr size_t bytes = smem_bytes<CHAR>();
+    auto kern = k_stage<RECON, CHAR, WZ, FLUX>;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)bytes);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    if (!a.uout) return cudaSuccess;  // configuration only (before graph capture)
+    dim3 grid((a.grid.ny + TY - 1) / TY, (a.grid.nx + TX - 1) / TX);
+    kern<<<grid, NT, bytes, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int RECON, bool CHAR, bool WZ>
+cudaError_t launch_flux(const StageArgs& a, cudaStream_t s) {
+    switch (a.num.flux) {
+        case FLUX_HLL: return launch_one<RECON, CHAR, WZ, FLUX_HLL>(a, s);
+        case FLUX_HLLC: return launch_one<RECON, CHAR, WZ, FLUX_HLLC>(a, s);
+        case FLUX_ROE: return launch_one<RECON, CHAR, WZ, FLUX_ROE>(a, s);
+        default: return launch_one<RECON, CHAR, WZ, FLUX_LLF>(a, s);
+    }
+}
+
+}  // namespace fp64stage
+
+cudaError_t launch_stage_fp64_w5(const StageArgs& a, cudaStream_t s);
+cudaError_t launch_stage_fp64_tvd(const StageArgs& a, cudaStream_t s);
+cudaError_t launch_stage_fp64_g1(const StageArgs& a, cudaStream_t s);
+
+}  // namespace eb2

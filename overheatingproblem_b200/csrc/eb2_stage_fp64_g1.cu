@@ -1,0 +1,11 @@
+// First-order (Godunov) instantiations of the FP64 fused stage, component and
+// characteristic (include/Reconstruction.h:51-239 of the reference).  Built
+// with -fmad=false: see eb2_point_fp64.cuh.
+#include "eb2_stage_fp64.cuh"
+
+namespace eb2 {
+cudaError_t launch_stage_fp64_g1(const StageArgs& a, cudaStream_t s) {
+    if (a.num.characteristic) return fp64stage::launch_flux<1, true, false>(a, s);
+    return fp64stage::launch_flux<1, false, false>(a, s);
+}
+}  // namespace eb2

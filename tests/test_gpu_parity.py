@@ -1,0 +1,221 @@
+"""GPU parity: libeuler_b200 against the reference's golden vectors and the
+CPU oracle, bit for bit (the FP64 form is compiled without FMA contraction and
+keeps the reference's evaluation order).  Corner ghost cells are excluded:
+no stencil reads them and the reference's outflow fills them in an
+order-dependent way."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GC, GOLDEN, bit_report, golden, interior, noncorner_mask, same_bits
+
+pytestmark = pytest.mark.gpu
+
+FQ = ["charjs_hllc_rk3", "comp_weno_hllc_rk3", "charz_roe_rk3", "charz_hll_rk2",
+      "comp_weno_llf_rk1", "tvd_char_hllc_rk3", "tvd_comp_roe_rk3", "godunov_char_hll_rk3",
+      "godunov_comp_hllc_rk1"]
+
+
+def make(gpu, nx, ny, **kw):
+    return gpu.Solver(nx, ny, **kw)
+
+
+@pytest.mark.parametrize("name", FQ)
+def test_rk_steps_bit_exact(gpu, name):
+    z = golden(f"fq_{name}")
+    with make(gpu, 32, 24, recon=int(z["recon"]), characteristic=bool(z["characteristic"]),
+              weno_z=bool(z["weno_z"])) as s:
+        s.init_case(gpu.lib.CASE_FOUR_QUADRANT)
+        U = s.download()
+        assert same_bits(interior(U), interior(z["U0"]))
+        for dt_ref in z["dts"]:
+            dt = s.delta_t(1 / 32, 1 / 24)
+            assert dt == dt_ref
+            s.rk_step(int(z["order"]), int(z["scheme"]), dt, 1 / 32, 1 / 24)
+        U = s.download()
+    m = noncorner_mask(U.shape)
+    assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
+
+
+def test_wall_heating_device_loop(gpu):
+    """The 400x8 wall-heating configuration run to t = 0.6 by the device time
+    loop (CUDA graphs): same step count, final time and bits as the reference."""
+    z = golden("wall_heating_400x8_t0.6")
+    with make(gpu, 400, 8, recon=5, characteristic=True, weno_z=False, cfl=0.5) as s:
+        lx, ly, tmax = s.init_case(gpu.lib.CASE_WALL_HEATING)
+        assert same_bits(s.download(), z["U0"])
+        n, tf = s.run(3, 2, lx / 400, ly / 8, tmax, n_out=1)
+        U = s.download()
+        assert s.status() == 0
+    assert n == int(z["steps"]) and tf == float(z["t_final"])
+    m = noncorner_mask(U.shape)
+    assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
+
+
+def test_double_mach_nonfinite_onset(gpu):
+    """The exact double-Mach boundary goes non-finite on the first step in the
+    reference; the GPU reproduces the same cells and flags it."""
+    z = golden("dmr_charjs_hllc_48x12_step1")
+    with make(gpu, 48, 12, recon=5, characteristic=True, weno_z=False, cfl=0.4) as s:
+        lx, ly, _ = s.init_case(gpu.lib.CASE_DOUBLE_MACH)
+        s.set_double_mach(True)
+        dt = s.delta_t(lx / 48, ly / 12)
+        assert dt == float(z["dt"])
+        rc = s.rk_step(3, 2, dt, lx / 48, ly / 12, 0.0)
+        assert rc == gpu.lib.EB2_ENONPHYS
+        assert s.status() & gpu.lib.ST_NONPHYSICAL
+        U = s.download()
+    assert same_bits(interior(U), interior(z["U"])), bit_report(interior(U), interior(z["U"]))
+
+
+def test_precision_known_answer(gpu):
+    with open(os.path.join(GOLDEN, "manifest.json")) as fh:
+        l1_ref = {int(k): v for k, v in json.load(fh)["precision"].items()}
+    l1 = {}
+    for nx in (10, 20, 40, 80):
+        z = golden(f"precision_nx{nx}")
+        with make(gpu, nx, 1, recon=5) as s:
+            lx, ly, tmax = s.init_case(gpu.lib.CASE_PRECISION)
+            assert same_bits(s.download(), z["U0"])
+            dx, dy = lx / nx, ly
+            t = 0.0
+            while t < tmax:
+                dt = 0.5 * dx ** (5.0 / 3)
+                if t + dt >= tmax:
+                    dt = tmax - t
+                s.rk_step(3, 2, dt, dx, dy)
+                t = t + dt
+            U = s.download()
+        assert same_bits(U[0, GC:-GC, GC], z["U"][0, GC:-GC, GC])
+        xc = (np.arange(nx) + 0.5) * dx
+        l1[nx] = float(np.sum(np.abs(1.0 + 0.2 * np.sin(xc - t) - U[0, GC:-GC, GC])) * dx)
+        assert l1[nx] == l1_ref[nx]
+    assert np.log2(l1[40] / l1[80]) > 4.5
+
+
+def test_granular_operators(gpu):
+    z = golden("granular_20x16")
+    dx, dy = 1 / 20, 1 / 16
+    with make(gpu, 20, 16, recon=5, characteristic=True, weno_z=True) as s:
+        s.upload(z["U"])
+        s.bc_apply()
+        Ub = s.download()
+        m = noncorner_mask(Ub.shape)
+        assert same_bits(Ub[:, m], z["Ub"][:, m])
+        s.upload(z["Ub"])
+        pri = s.con_to_pri()
+        box = (slice(None), slice(GC - 1, -GC + 1), slice(GC - 1, -GC + 1))
+        assert same_bits(pri[box], z["pri"][box])
+        assert s.delta_t(dx, dy) == float(z["dt"])
+        for d in (1, 2):
+            el, er = s.eigen(d, z["pri"])
+            sl = (slice(None), slice(None), slice(GC - 1, -GC), slice(GC, -GC)) if d == 1 else \
+                 (slice(None), slice(None), slice(GC, -GC), slice(GC - 1, -GC))
+            assert same_bits(el[sl], z[f"eig_l{d}"][sl])
+            assert same_bits(er[sl], z[f"eig_r{d}"][sl])
+            face = (slice(None), slice(GC - 1, -GC), slice(GC, -GC)) if d == 1 else \
+                   (slice(None), slice(GC, -GC), slice(GC - 1, -GC))
+            for tag, (recon, ch, wz) in {"charz": (5, 1, 1), "charjs": (5, 1, 0),
+                                         "comp": (5, 0, 1), "tvdc": (2, 1, 1), "tvdm": (2, 0, 1),
+                                         "god": (1, 1, 1)}.items():
+                s.set_reconstruction(recon, ch, wz)
+                ql, qr = s.reconstruct(d, dx, dy)
+                assert same_bits(ql[face], z[f"ql_{tag}{d}"][face]), tag
+                assert same_bits(qr[face], z[f"qr_{tag}{d}"][face]), tag
+            for scheme in (1, 2, 3, 4):
+                fl = s.riemann(scheme, d, z[f"ql_charz{d}"], z[f"qr_charz{d}"])
+                assert same_bits(fl[face], z[f"flux{scheme}_{d}"][face]), (scheme, d)
+        s.set_reconstruction(5, True, True)
+        f, g = s.flux_reconstruction(2, dx, dy)
+        fx = (slice(None), slice(GC - 1, -GC), slice(GC, -GC))
+        gy = (slice(None), slice(GC, -GC), slice(GC - 1, -GC))
+        assert same_bits(f[fx], z["f"][fx]) and same_bits(g[gy], z["g"][gy])
+        Lt = s.space_discrete(dx, dy, z["f"], z["g"])
+        assert same_bits(interior(Lt), interior(z["L"]))
+
+
+def test_boundary_kinds(gpu):
+    z = golden("boundary_12x10")
+    for key in z.files:
+        U, Ub = z[key][0], z[key][1]
+        with make(gpu, 12, 10) as s:
+            s.upload(U)
+            if key == "bc_dmr_t0.05":
+                s.set_double_mach(True)
+                s.bc_apply(0.05)
+            else:
+                k = [int(c) for c in key[3:]]
+                s.set_bc(*k)
+                s.bc_apply()
+            out = s.download()
+        m = noncorner_mask(out.shape)
+        assert same_bits(out[:, m], Ub[:, m]), (key, bit_report(out[:, m], Ub[:, m]))
+
+
+@pytest.mark.parametrize("case", [0, 1, 4, 6, 7, 8, 9, 10, 11, 16])
+def test_reference_initial_states(gpu, case):
+    z = golden("init_cases")
+    U_ref, meta = z[f"case{case}"], z[f"case{case}_meta"]
+    nx, ny = U_ref.shape[1] - 2 * GC, U_ref.shape[2] - 2 * GC
+    with make(gpu, nx, ny) as s:
+        lx, ly, tmax = s.init_case(case)
+        U = s.download()
+    assert (lx, ly, tmax) == tuple(meta[:3])
+    if case in (0, 16):  # interior-only initialisers
+        assert same_bits(interior(U), interior(U_ref))
+    else:
+        assert same_bits(U, U_ref), bit_report(U, U_ref)
+
+
+@pytest.mark.parametrize("scheme", [1, 2, 3, 4])
+@pytest.mark.parametrize("kinds", [(1, 0, 2, 2), (2, 2, 1, 1), (3, 0, 1, 0)])
+def test_random_state_against_oracle(gpu, oracle, kinds, scheme):
+    """Mixed boundaries on a smooth random state, characteristic WENO5-JS."""
+    nx, ny = 37, 29   # not multiples of the 16 x 32 tile
+    p = oracle.params(nx, ny, recon=5, characteristic=1, weno_z=0, bc=kinds)
+    rng = np.random.default_rng(100 + scheme)
+    x = np.linspace(0, 2 * np.pi, nx)[:, None]
+    y = np.linspace(0, 2 * np.pi, ny)[None, :]
+    W = np.zeros((4, nx + 8, ny + 8))
+    W[0, GC:-GC, GC:-GC] = 1.0 + 0.3 * np.sin(x) * np.cos(y) + 0.05 * rng.random((nx, ny))
+    W[1, GC:-GC, GC:-GC] = 0.4 * np.cos(x + y)
+    W[2, GC:-GC, GC:-GC] = -0.3 * np.sin(2 * y) + 0.1 * rng.random((nx, ny))
+    W[3, GC:-GC, GC:-GC] = 1.0 + 0.2 * np.cos(x - y)
+    U = np.zeros_like(W)
+    U[0], U[1], U[2] = W[0], W[1] * W[0], W[2] * W[0]
+    U[3] = W[3] / 0.4 + 0.5 * W[0] * (W[1] ** 2 + W[2] ** 2)
+    Ua = U.copy()
+    with make(gpu, nx, ny, recon=5, characteristic=True, weno_z=False) as s:
+        s.set_bc(*kinds)
+        s.upload(U)
+        for _ in range(3):
+            dt = oracle.dt(p, Ua, 1 / nx, 1 / ny)
+            assert s.delta_t(1 / nx, 1 / ny) == dt
+            oracle.rk(p, 3, scheme, Ua, dt, 1 / nx, 1 / ny)
+            s.rk_step(3, scheme, dt, 1 / nx, 1 / ny)
+        Ub = s.download()
+    m = noncorner_mask(U.shape)
+    assert same_bits(Ua[:, m], Ub[:, m]), bit_report(Ua[:, m], Ub[:, m])
+
+
+def test_device_loop_matches_host_loop(gpu, oracle):
+    """eb2_run (device time loop, outputs paused at 3 output times) against the
+    oracle's host loop on the four-quadrant problem, 96 x 80 to t = 0.05."""
+    nx, ny = 96, 80
+    p = oracle.params(nx, ny, recon=5, characteristic=1, weno_z=0, cfl=0.5)
+    U0, lx, ly, _ = oracle.init_case(p, 1)
+    Ua = U0.copy()
+    na, ta = oracle.run(p, 3, 2, Ua, lx / nx, ly / ny, 0.05, 3)
+    seen = []
+    with make(gpu, nx, ny, recon=5, characteristic=True, weno_z=False) as s:
+        s.init_case(gpu.lib.CASE_FOUR_QUADRANT)
+        nb, tb = s.run(3, 2, lx / nx, ly / ny, 0.05, n_out=3,
+                       on_output=lambda t, k: seen.append((t, k)))
+        Ub = s.download()
+    assert (na, ta) == (nb, tb)
+    assert len(seen) == 3 and abs(seen[-1][0] - 0.05) < 1e-15
+    assert same_bits(interior(Ua), interior(Ub)), bit_report(interior(Ua), interior(Ub))
