@@ -20,11 +20,16 @@ Our arm prints one JSON line with
             RK3 step: 64 + 96 + 96) over its measured device time, against the
             measured copy bandwidth;
   cpu_baseline  the reference built from its own sources (oracle/_ref), all
-            host cores, on a bounded sample of the same workload.
+            host cores, on a bounded sample of the same workload;
+  extra     the same device-time measurement for the 4096^2 grid in the FP64
+            and mixed-precision forms (HLLC and Roe).
 With --impl reference, rank 0 times the reference's CPU implementation on the
 same workload and prints the reference line; other ranks exit.
 For N > 1 (torchrun) every rank runs an independent replica (weak scaling):
 a single solve of this size does not shard in this build.
+
+--nx/--precision/--scheme/--no-e2e/--no-cpu-baseline/--no-extra select a single
+measurement (used for profiling runs).
 """
 from __future__ import annotations
 
@@ -40,33 +45,41 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NX = NY = 1024
-ORDER, SCHEME = 3, 2          # SSP-RK3, HLLC
+ORDER = 3                     # SSP-RK3
+SCHEMES = {"hllc": 2, "roe": 3, "hll": 1, "llf": 4}
 BYTES_PER_CELL_STEP = 256     # 64 + 96 + 96 algorithmic HBM bytes (FP64 state)
 FLUSH_BYTES = 256 << 20       # > 126 MB L2
 METRIC = "cell-updates/s"
-WORKLOAD = "four-quadrant Riemann 1024x1024, characteristic WENO5-JS + HLLC + SSP-RK3, FP64"
 FALLBACK_HBM_GBS = 6650.0
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--scheme", choices=sorted(SCHEMES), default="hllc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true")
     return ap.parse_args()
 
 
-def config(extra=None):
-    c = {"workload": WORKLOAD, "nx": NX, "ny": NY, "order": ORDER, "scheme": "HLLC",
-         "reconstruction": "WENO5-JS characteristic", "cfl": 0.5, "dtype": "f64",
-         "l2": "flushed between timed steps (256 MiB write outside the timed intervals)",
-         "parallelism": "replicas"}
-    if extra:
-        c.update(extra)
-    return c
+def workload(nx, precision, scheme):
+    return (f"four-quadrant Riemann {nx}x{nx}, characteristic WENO5-JS + {scheme.upper()} + "
+            f"SSP-RK3, {'FP64' if precision == 'fp64' else 'mixed FP32/FP64'}")
+
+
+def config(args):
+    return {"workload": workload(args.nx, args.precision, args.scheme), "nx": args.nx,
+            "ny": args.nx, "order": ORDER, "scheme": args.scheme.upper(),
+            "reconstruction": "WENO5-JS characteristic", "cfl": 0.5,
+            "precision": args.precision,
+            "l2": "flushed between timed steps (256 MiB write outside the timed intervals)",
+            "parallelism": "replicas"}
 
 
 def hbm_peak():
@@ -91,7 +104,7 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(gpu_index)], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "-lms", "100", "-i", str(gpu_index)], stdout=self.fh, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
@@ -127,7 +140,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- dist
-def dist_setup(n, collective=True):
+def dist_setup(collective=True):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -177,41 +190,42 @@ def reference_lib():
     return Oracle(), "port"
 
 
-def cpu_rate(budget_s: float, max_steps: int, warmup: int):
+def cpu_rate(nx: int, scheme: int, budget_s: float, max_steps: int, warmup: int):
     """Cell-updates/s of the CPU implementation on the benchmark workload:
-    full 1024^2 RK3 steps until the time budget is spent."""
+    full nx^2 RK3 steps until the time budget is spent."""
     from oracle.bind import FOUR_QUADRANT, Oracle
     lib, kind = reference_lib()
     orc = Oracle()
-    p = orc.params(NX, NY, recon=5, characteristic=1, weno_z=0, cfl=0.5)
+    p = orc.params(nx, nx, recon=5, characteristic=1, weno_z=0, cfl=0.5)
     U, lx, ly, _ = orc.init_case(p, FOUR_QUADRANT)
-    dx, dy = lx / NX, ly / NY
+    dx, dy = lx / nx, ly / nx
     for _ in range(warmup):
-        lib.rk(p, ORDER, SCHEME, U, lib.dt(p, U, dx, dy), dx, dy)
+        lib.rk(p, ORDER, scheme, U, lib.dt(p, U, dx, dy), dx, dy)
     n, t0 = 0, time.perf_counter()
-    while n < max_steps:
+    while n < max(1, max_steps):
         dt = lib.dt(p, U, dx, dy)
-        lib.rk(p, ORDER, SCHEME, U, dt, dx, dy)
+        lib.rk(p, ORDER, scheme, U, dt, dx, dy)
         n += 1
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return NX * NY * n / el, el / n, n, kind, cores
+    return nx * nx * n / el, el / n, n, kind, cores
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     # bounded: at most ~150 s of timed CPU work whatever K is
-    rate, per_step, n, kind, cores = cpu_rate(150.0, args.steps, min(args.warmup, 1))
+    rate, per_step, n, kind, cores = cpu_rate(args.nx, SCHEMES[args.scheme], 150.0, args.steps,
+                                              min(args.warmup, 1))
     line = {
         "metric": METRIC, "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
         "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": per_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config(), "impl": "reference",
+        "data": "synthetic", "config": config(args), "impl": "reference",
         "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": kind,
-                         "sample": f"{n} full SSP-RK3 steps of the 1024^2 grid"},
+                         "sample": f"{n} full SSP-RK3 steps of the {args.nx}^2 grid"},
         "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -219,78 +233,108 @@ def run_reference(args, world, rank):
 
 
 # --------------------------------------------------------------------------- GPU
+def measure(eb2, local, nx, precision, scheme, steps, warmup, flush=FLUSH_BYTES):
+    """Device time of `steps` steps (after `warmup`), L2 flushed between steps."""
+    prec = eb2.lib.FP64 if precision == "fp64" else eb2.lib.MIXED
+    s = eb2.Solver(nx, nx, device=local, recon=5, characteristic=True, weno_z=False, cfl=0.5,
+                   precision=prec)
+    lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    dx, dy = lx / nx, ly / nx
+    if warmup:
+        s.bench_steps(ORDER, scheme, dx, dy, warmup, 0)
+        s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    step_ms, stage_ms, nstage, launches = s.bench_steps(ORDER, scheme, dx, dy, steps, flush)
+    st = s.status()
+    return s, dx, dy, step_ms, stage_ms, nstage, launches, st
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
 
     import overheatingproblem_b200 as eb2
 
-    s = eb2.Solver(NX, NY, device=local, recon=5, characteristic=True, weno_z=False, cfl=0.5)
-    lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
-    dx, dy = lx / NX, ly / NY
-    # warm-up (kernel attributes, clocks)
-    s.bench_steps(ORDER, SCHEME, dx, dy, max(args.warmup, 3), 0)
-    s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    nx, scheme = args.nx, SCHEMES[args.scheme]
+    torch.cuda.init()
+    # warm-up pass (clocks, kernel attributes) outside the timed region
+    s, *_ = measure(eb2, local, nx, args.precision, scheme, max(args.warmup, 3), 0, 0)
+    s.close()
     torch.cuda.synchronize(local)
     sampler = ClockSampler(physical_gpu(local)) if rank == 0 else None
     barrier(world)
     torch.cuda.synchronize(local)
-    step_ms, stage_ms, nstage, launches = s.bench_steps(ORDER, SCHEME, dx, dy, args.steps,
-                                                        FLUSH_BYTES)
+    s, dx, dy, step_ms, stage_ms, nstage, launches, st = measure(
+        eb2, local, nx, args.precision, scheme, args.steps, 0)
     torch.cuda.synchronize(local)
     barrier(world)
     clocks = sampler.stop() if sampler else None
-    st = s.status()
     total_ms = allreduce_max(float(sum(step_ms)), world)
-    value = world * NX * NY * args.steps / (total_ms * 1e-3)
+    value = world * nx * nx * args.steps / (total_ms * 1e-3)
 
-    # roofline of the fused stage kernel
     peak, peak_kind = hbm_peak()
-    alg_bytes = NX * NY * BYTES_PER_CELL_STEP * args.steps
+    alg_bytes = nx * nx * BYTES_PER_CELL_STEP * args.steps
     achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None,
-                "kernel": "eb2::fp64stage::k_stage (fused x+y sweep + RK stage)",
+                "kernel": f"eb2 fused x+y sweep + RK stage ({args.precision})",
                 "per_launch_ms": stage_ms / nstage, "peak_kind": peak_kind,
-                "alg_bytes_per_launch": NX * NY * BYTES_PER_CELL_STEP / ORDER}
+                "alg_bytes_per_launch": nx * nx * BYTES_PER_CELL_STEP / ORDER,
+                "stage_share_of_step": stage_ms / sum(step_ms)}
 
-    # end to end through the C ABI with host buffers
-    s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
-    host = torch.empty((4, NX + 8, NY + 8), dtype=torch.float64, pin_memory=True).numpy()
-    s.download(host)
-    k_e2e = max(3, min(args.steps, 50))
-    for _ in range(2):
-        s.upload(host)
-        dt = s.delta_t(dx, dy)
-        s.rk_step(ORDER, SCHEME, dt, dx, dy)
+    e2e = None
+    if not args.no_e2e:
+        s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+        host = torch.empty((4, nx + 8, nx + 8), dtype=torch.float64, pin_memory=True).numpy()
         s.download(host)
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        s.upload(host)
-        dt = s.delta_t(dx, dy)
-        s.rk_step(ORDER, SCHEME, dt, dx, dy)
-        s.download(host)
-    e2e_s = allreduce_max(time.perf_counter() - t0, world)
-    e2e = {"value": world * NX * NY * k_e2e / e2e_s, "unit": "cell-updates/s",
-           "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes) + 8,
-           "steps": k_e2e, "path": "eb2_upload + eb2_delta_t + eb2_rk_step + eb2_download"}
+        k_e2e = max(3, min(args.steps, 50))
+        for _ in range(2):
+            s.upload(host)
+            s.rk_step(ORDER, scheme, s.delta_t(dx, dy), dx, dy)
+            s.download(host)
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            s.upload(host)
+            dt = s.delta_t(dx, dy)
+            s.rk_step(ORDER, scheme, dt, dx, dy)
+            s.download(host)
+        e2e_s = allreduce_max(time.perf_counter() - t0, world)
+        e2e = {"value": world * nx * nx * k_e2e / e2e_s, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes) + 8,
+               "steps": k_e2e, "timer": "host wall clock, max over ranks",
+               "path": "eb2_upload + eb2_delta_t + eb2_rk_step + eb2_download"}
     s.close()
+
+    extra = {}
+    if not args.no_extra:
+        for tag, (n2, prec, sch, k) in {
+                "fp64_4096_hllc": (4096, "fp64", 2, 10),
+                "mixed_4096_hllc": (4096, "mixed", 2, 40),
+                "mixed_4096_roe": (4096, "mixed", 3, 40),
+                "mixed_1024_hllc": (1024, "mixed", 2, 200)}.items():
+            s2, _, _, sm, stm, nst, _, st2 = measure(eb2, local, n2, prec, sch, k, 2)
+            s2.close()
+            tot = allreduce_max(float(sum(sm)), world)
+            extra[tag] = {"value": world * n2 * n2 * k / (tot * 1e-3), "unit": "cell-updates/s",
+                          "ms_per_step": tot / k, "steps": k, "status_flags": st2,
+                          "roofline_frac": n2 * n2 * BYTES_PER_CELL_STEP * k / (stm * 1e-3) / 1e9
+                          / peak}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, per_step, n, kind, cores = cpu_rate(20.0, 40, 1)
+        rate, per_step, n, kind, cores = cpu_rate(nx, scheme, 20.0, 40, 1)
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": kind,
-               "sample": f"{n} full SSP-RK3 steps of the 1024^2 grid ({per_step:.3f} s each)"}
+               "sample": f"{n} full SSP-RK3 steps of the {nx}^2 grid ({per_step:.3f} s each)"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(args),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "status_flags": st,
             "step_ms_min_median_max": [min(step_ms), float(np.median(step_ms)), max(step_ms)],
+            "extra": extra,
         }
         print(json.dumps(line), flush=True)
 
@@ -298,7 +342,7 @@ def run_ours(args, world, rank, local):
 def main():
     args = parse()
     # the reference arm uses no collective: rank 0 works, the others leave
-    world, rank, local = dist_setup(args.gpus, collective=args.impl == "ours")
+    world, rank, local = dist_setup(collective=args.impl == "ours")
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)

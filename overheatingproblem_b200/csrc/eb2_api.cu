@@ -602,6 +602,13 @@ int eb2_rk_step(eb2_ctx* c, int order, int scheme, double dt, double dx, double 
     set_spacing(c, dx, dy);
     unsigned before = 0, after = 0;
     if (int r = read_status(c, &before)) return r;
+    if (c->precision == EB2_MIXED) {
+        // the near-vacuum threshold of the mixed form needs the mean pressure
+        int nb = 0;
+        CK(launch_wave_partials(c->u, c->grid, c->gas, c->partials, &nb, c->stream));
+        CK(launch_finalize(c->ctrl, c->partials, nb, c->grid.nx * c->grid.ny, 0, c->stream));
+        c->launches += 2;
+    }
     k_set_step<<<1, 1, 0, c->stream>>>(c->ctrl, time, dt);
     CK(cudaGetLastError());
     CK(enqueue_step(c, order));

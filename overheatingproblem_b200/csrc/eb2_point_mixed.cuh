@@ -1,0 +1,346 @@
+// eb2_point_mixed.cuh -- per-interface arithmetic of the mixed-precision form.
+//
+// The conserved state, the RK stage sums and the CFL reduction stay FP64; the
+// characteristic projection, WENO5 reconstruction and Riemann flux run in
+// FP32 with three reformulations that keep FP32 rounding relative to the
+// quantities that matter rather than to |U|:
+//
+//  * delta form -- the stencil is projected as differences from the cell
+//    next to the interface (the "base" cell), so rounding is relative to the
+//    jumps; WENO is translation invariant, the base is added back after the
+//    back-projection;
+//  * cancellation-free thermodynamics -- the Roe sound speed is formed from
+//    h = gamma/(gamma-1) p/rho of each cell plus 1/2 wa wb |du|^2 instead of
+//    H - q^2/2, b2 = b1 q^2 / 2, and interface pressures are p_base +
+//    (gamma-1)(dE - dK) with dK the kinetic-energy change written in
+//    differences; cell pressures themselves come from FP64;
+//  * rescaled epsilon -- the WENO weights are formed with one reciprocal per
+//    side from products of (beta + eps)^2 after scaling the stencil by a power
+//    of two; the reference's absolute eps = 1e-15 (Reconstruction.h:1414)
+//    becomes a relative floor eps = 1e-6 * s^2, s the stencil's largest
+//    difference, above FP32 rounding noise.
+// Interfaces next to near-vacuum cells (p < 1e-3 of the mean pressure) get
+// their Roe eigenvectors from FP64 arithmetic.
+#pragma once
+
+#include "eb2_common.cuh"
+
+namespace eb2 {
+namespace f32 {
+
+__device__ __forceinline__ float rcp(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsq(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqr(float x) { return x * rsq(x); }  // sqrt for x > 0
+
+// Per-cell primitive data kept in shared memory (FP32 values of FP64 results).
+enum : int { P_RHO = 0, P_U = 1, P_V = 2, P_P = 3, P_H = 4, P_SR = 5, NP = 6 };
+
+// Eigen-system parameters at an interface (the Roe average), in the form the
+// factored projections below use.
+struct Eig {
+    float u, v, c, hb1, hic, hq2, cg, b1, H;
+};
+
+__device__ __forceinline__ Eig eig_from(float u, float v, float c2, float gm1) {
+    Eig e;
+    float ic = rsq(c2);
+    e.u = u;
+    e.v = v;
+    e.c = c2 * ic;
+    float b1 = gm1 * ic * ic;
+    float q2 = u * u + v * v;
+    e.b1 = b1;
+    e.hb1 = 0.5f * b1;
+    e.hic = 0.5f * ic;
+    e.hq2 = 0.5f * q2;
+    e.cg = c2 * (1.0f / gm1);
+    e.H = e.cg + e.hq2;
+    return e;
+}
+
+// Roe average from FP32 cell data: weights sqrt(rho), sound speed from the
+// cell enthalpies h (no H - q^2/2 cancellation).
+__device__ __forceinline__ Eig roe_f32(const float* a, const float* b, int ps, float gm1) {
+    float sa = a[P_SR * ps], sb = b[P_SR * ps];
+    float rs = rcp(sa + sb);
+    float wa = sa * rs, wb = sb * rs;
+    float ua = a[P_U * ps], ub = b[P_U * ps], va = a[P_V * ps], vb = b[P_V * ps];
+    float u = wa * ua + wb * ub;
+    float v = wa * va + wb * vb;
+    float du = ua - ub, dv = va - vb;
+    float h = wa * a[P_H * ps] + wb * b[P_H * ps];
+    float c2 = gm1 * (h + 0.5f * wa * wb * (du * du + dv * dv));
+    return eig_from(u, v, c2, gm1);
+}
+
+// The same average in FP64 from the cells' FP64 conserved states (near-vacuum
+// interfaces): the reference's own formulas (Characteriz.h:333-342).
+__device__ __forceinline__ Eig roe_f64(const double* qa, const double* qb, double gm1,
+                                       double gr) {
+    double ua = qa[1] / qa[0], va = qa[2] / qa[0];
+    double ub = qb[1] / qb[0], vb = qb[2] / qb[0];
+    double pa = (qa[3] - 0.5 * qa[0] * (ua * ua + va * va)) * gm1;
+    double pb = (qb[3] - 0.5 * qb[0] * (ub * ub + vb * vb)) * gm1;
+    double Ha = 0.5 * (ua * ua + va * va) + gr * (pa / qa[0]);
+    double Hb = 0.5 * (ub * ub + vb * vb) + gr * (pb / qb[0]);
+    double D = sqrt(qb[0] / qa[0]);
+    double D1 = D + 1.0;
+    double u = (ua + D * ub) / D1, v = (va + D * vb) / D1, H = (Ha + D * Hb) / D1;
+    double c2 = gm1 * (H - 0.5 * (u * u + v * v));
+    Eig e;
+    double c = sqrt(c2);
+    e.u = (float)u;
+    e.v = (float)v;
+    e.c = (float)c;
+    e.b1 = (float)(gm1 / c2);
+    e.hb1 = 0.5f * e.b1;
+    e.hic = (float)(0.5 / c);
+    e.hq2 = (float)(0.5 * (u * u + v * v));
+    e.cg = (float)(c2 / gm1);
+    e.H = (float)H;
+    return e;
+}
+
+// Characteristic variables of a conserved difference d (left-eigenvector rows
+// of Characteriz.h:346-367 / :448-469 in factored form).
+template <int DIR>
+__device__ __forceinline__ void project(const Eig& e, float d0, float d1, float d2, float d3,
+                                        float* w) {
+    float K = fmaf(e.hq2, d0, d3);
+    K = fmaf(-e.u, d1, K);
+    K = fmaf(-e.v, d2, K);
+    float A = DIR == 1 ? fmaf(e.u, d0, -d1) : fmaf(e.v, d0, -d2);
+    float bK = e.hb1 * K, cA = e.hic * A;
+    w[0] = bK + cA;
+    w[3] = bK - cA;
+    w[1] = fmaf(e.cg, d0, -K);
+    w[2] = DIR == 1 ? fmaf(e.v, d0, -d2) : fmaf(-e.u, d0, d1);
+}
+
+// Conserved difference from characteristic values (right eigenvectors,
+// Characteriz.h:371-392 / :473-494, factored).
+template <int DIR>
+__device__ __forceinline__ void unproject(const Eig& e, const float* w, float* q) {
+    float S = fmaf(e.b1, w[1], w[0] + w[3]);
+    float D = w[0] - w[3];
+    float cD = e.c * D;
+    q[0] = S;
+    if (DIR == 1) {
+        q[1] = fmaf(e.u, S, -cD);
+        q[2] = fmaf(e.v, S, -w[2]);
+        q[3] = fmaf(e.H, S, fmaf(-e.u, cD, fmaf(-e.v, w[2], -w[1])));
+    } else {
+        q[1] = fmaf(e.u, S, w[2]);
+        q[2] = fmaf(e.v, S, -cD);
+        q[3] = fmaf(e.H, S, fmaf(-e.v, cD, fmaf(e.u, w[2], -w[1])));
+    }
+}
+
+// WENO5 at both sides of an interface from the six characteristic values
+// w[0..5] (cells i-2..i+3) with w[2] == 0 (delta form around cell i).
+// Returns the minus-side value (WENO5_L on i-2..i+2) and the plus-side value
+// (WENO5_R on i+3..i-1).  WZ selects WENO-Z weights.
+template <bool WZ>
+__device__ __forceinline__ void weno5_pair(float w0, float w1, float w3, float w4, float w5,
+                                           float& qm, float& qp) {
+    // power-of-two scale of the stencil, so that the products below stay in range
+    float s = fmaxf(fmaxf(fmaxf(fabsf(w0), fabsf(w1)), fmaxf(fabsf(w3), fabsf(w4))), fabsf(w5));
+    if (!(s > 0.0f)) {  // flat (or non-finite) stencil
+        qm = qp = (s == 0.0f) ? 0.0f : s;
+        return;
+    }
+    // 2^-e with s = m * 2^e, m in [1, 2): exact scaling
+    float sc = __int_as_float((254 - ((__float_as_int(s) >> 23) & 0xff)) << 23);
+    float sc2 = sc * sc;
+    const float k13 = 13.0f / 12.0f, eps = 1.0e-6f;
+    // second differences shared by both sides
+    float a1 = fmaf(-2.0f, w1, w0);          // w0 - 2 w1 + w2
+    float a2 = w1 + w3;                      // w1 - 2 w2 + w3
+    float a3 = fmaf(-2.0f, w3, w4);          // w2 - 2 w3 + w4
+    float a4 = fmaf(-2.0f, w4, w5 + w3);     // w3 - 2 w4 + w5
+    float A1 = k13 * a1 * a1, A2 = k13 * a2 * a2, A3 = k13 * a3 * a3, A4 = k13 * a4 * a4;
+    float bl1 = fmaf(-4.0f, w1, w0);         // w0 - 4 w1 + 3 w2
+    float bl2 = w1 - w3;                     // w1 - w3
+    float bl3 = fmaf(-4.0f, w3, w4);         // 3 w2 - 4 w3 + w4
+    float br1 = fmaf(-4.0f, w4, fmaf(3.0f, w3, w5));  // w5 - 4 w4 + 3 w3
+    float br2 = w4;                          // w4 - w2
+    float br3 = fmaf(3.0f, w3, w1);          // 3 w3 - 4 w2 + w1
+    float bL1 = fmaf(0.25f * bl1, bl1, A1), bL2 = fmaf(0.25f * bl2, bl2, A2);
+    float bL3 = fmaf(0.25f * bl3, bl3, A3);
+    float bR1 = fmaf(0.25f * br1, br1, A4), bR2 = fmaf(0.25f * br2, br2, A3);
+    float bR3 = fmaf(0.25f * br3, br3, A2);
+    // candidate stencil values times 6 (Reconstruction.h:1452-1454 with w2 = 0)
+    float cl1 = fmaf(2.0f, w0, -7.0f * w1);
+    float c2 = fmaf(2.0f, w3, -w1);          // left candidate 2 == right candidate 3
+    float c3 = fmaf(5.0f, w3, -w4);          // left candidate 3 == right candidate 2
+    float cr1 = fmaf(2.0f, w5, fmaf(-7.0f, w4, 11.0f * w3));
+    auto side = [&](float b1, float b2, float b3, float k1, float k2, float k3) {
+        float t1 = fmaf(b1, sc2, eps), t2 = fmaf(b2, sc2, eps), t3 = fmaf(b3, sc2, eps);
+        float g1, g2, g3;
+        if (WZ) {
+            // WENO-Z (Reconstruction.h:1546-1551): a_k = d_k (1 + tau5 / (beta_k + eps))
+            float tau = fabsf(t1 - t3);
+            float p23 = t2 * t3, p13 = t1 * t3, p12 = t1 * t2;
+            g1 = 0.1f * (p23 * t1 + tau * p23);
+            g2 = 0.6f * (p13 * t2 + tau * p13);
+            g3 = 0.3f * (p12 * t3 + tau * p12);
+        } else {
+            float q1 = t1 * t1, q2 = t2 * t2, q3 = t3 * t3;
+            g1 = 0.1f * (q2 * q3);
+            g2 = 0.6f * (q1 * q3);
+            g3 = 0.3f * (q1 * q2);
+        }
+        float r = rcp(g1 + g2 + g3) * (1.0f / 6.0f);
+        return fmaf(g1, k1, fmaf(g2, k2, g3 * k3)) * r;
+    };
+    qm = side(bL1, bL2, bL3, cl1, c2, c3);
+    qp = side(bR1, bR2, bR3, cr1, c3, c2);
+}
+
+// Interface state in primitive form from the base cell and a conserved
+// difference (no cancellation: see the file comment).
+struct Prim {
+    float r, un, ut, p, E, ir;
+};
+
+template <int DIR>
+__device__ __forceinline__ Prim prim_from_delta(float rb, float ub, float vb, float pb, float Eb,
+                                                const float* dq, float gm1) {
+    Prim s;
+    float r = rb + dq[0];
+    float ir = rcp(r);
+    float u = fmaf(fmaf(-ub, dq[0], dq[1]), ir, ub);
+    float v = fmaf(fmaf(-vb, dq[0], dq[2]), ir, vb);
+    // dK = [rb (2 ub.dm - drho |ub|^2) + |dm|^2] / (2 r)
+    float udm = fmaf(ub, dq[1], vb * dq[2]);
+    float t = fmaf(rb, fmaf(2.0f, udm, -dq[0] * fmaf(ub, ub, vb * vb)),
+                   fmaf(dq[1], dq[1], dq[2] * dq[2]));
+    float dK = 0.5f * t * ir;
+    s.r = r;
+    s.ir = ir;
+    s.p = fmaf(gm1, dq[3] - dK, pb);
+    s.E = Eb + dq[3];
+    s.un = DIR == 1 ? u : v;
+    s.ut = DIR == 1 ? v : u;
+    return s;
+}
+
+// Physical flux in (mass, normal momentum, tangential momentum, energy) order.
+__device__ __forceinline__ void pflux(const Prim& s, float* F) {
+    float m = s.r * s.un;
+    F[0] = m;
+    F[1] = fmaf(m, s.un, s.p);
+    F[2] = m * s.ut;
+    F[3] = (s.E + s.p) * s.un;
+}
+
+// HLLC with Einfeldt speeds (include/scheme.h:690-1001, sound speed
+// sqrt(gamma p / rho) on both sweeps).
+__device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float gamma, float* F) {
+    float aL2 = gamma * L.p * L.ir, aR2 = gamma * R.p * R.ir;
+    float sqL = sqr(L.r), sqR = sqr(R.r);
+    float is = rcp(sqL + sqR);
+    float nbar = (sqL * L.un + sqR * R.un) * is;
+    float eta = 0.5f * sqL * sqR * is * is;
+    float du = R.un - L.un;
+    float dd2 = fmaf((sqL * aL2 + sqR * aR2), is, eta * du * du);
+    float dd = sqr(dd2);
+    float sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0f) {
+        pflux(L, F);
+        return;
+    }
+    if (sr <= 0.0f) {
+        pflux(R, F);
+        return;
+    }
+    float mL = L.r * (sl - L.un), mR = R.r * (sr - R.un);
+    float ss = (R.p - L.p + L.un * mL - R.un * mR) * rcp(mL - mR);
+    const Prim& S = ss >= 0.0f ? L : R;
+    float sk = ss >= 0.0f ? sl : sr;
+    float mk = ss >= 0.0f ? mL : mR;
+    float Fk[4];
+    pflux(S, Fk);
+    float f = mk * rcp(sk - ss);                      // star density
+    float e = S.E * S.ir + (ss - S.un) * (ss + S.p * rcp(mk));
+    F[0] = fmaf(sk, f - S.r, Fk[0]);
+    F[1] = fmaf(sk, fmaf(f, ss, -S.r * S.un), Fk[1]);
+    F[2] = fmaf(sk, fmaf(f, S.ut, -S.r * S.ut), Fk[2]);
+    F[3] = fmaf(sk, fmaf(f, e, -S.E), Fk[3]);
+}
+
+// HLL with Einfeldt speeds (include/scheme.h:400-674).
+__device__ __forceinline__ void hll(const Prim& L, const Prim& R, float gamma, float* F) {
+    float aL2 = gamma * L.p * L.ir, aR2 = gamma * R.p * R.ir;
+    float sqL = sqr(L.r), sqR = sqr(R.r);
+    float is = rcp(sqL + sqR);
+    float nbar = (sqL * L.un + sqR * R.un) * is;
+    float eta = 0.5f * sqL * sqR * is * is;
+    float du = R.un - L.un;
+    float dd = sqr(fmaf((sqL * aL2 + sqR * aR2), is, eta * du * du));
+    float sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0f) { pflux(L, F); return; }
+    if (sr <= 0.0f) { pflux(R, F); return; }
+    float FL[4], FR[4];
+    pflux(L, FL);
+    pflux(R, FR);
+    float UL[4] = {L.r, L.r * L.un, L.r * L.ut, L.E}, UR[4] = {R.r, R.r * R.un, R.r * R.ut, R.E};
+    float id = rcp(sr - sl), slsr = sl * sr;
+#pragma unroll
+    for (int k = 0; k < 4; k++) F[k] = (sr * FL[k] - sl * FR[k] + slsr * (UR[k] - UL[k])) * id;
+}
+
+// Roe flux with |lambda| (include/scheme.h:1018-1322), normal-aligned.
+__device__ __forceinline__ void roe(const Prim& L, const Prim& R, float gamma, float* F) {
+    float gm1 = gamma - 1.0f;
+    float sqL = sqr(L.r), sqR = sqr(R.r);
+    float is = rcp(sqL + sqR);
+    float wa = sqL * is, wb = sqR * is;
+    float un = wa * L.un + wb * R.un, ut = wa * L.ut + wb * R.ut;
+    float dun = R.un - L.un, dut = R.ut - L.ut;
+    float hL = gamma / gm1 * L.p * L.ir, hR = gamma / gm1 * R.p * R.ir;
+    float c2 = gm1 * (wa * hL + wb * hR + 0.5f * wa * wb * (dun * dun + dut * dut));
+    float ic = rsq(c2), c = c2 * ic;
+    float q2 = un * un + ut * ut;
+    float H = c2 / gm1 + 0.5f * q2;
+    float rbar = sqL * sqR;
+    float dp = R.p - L.p, drho = R.r - L.r;
+    float ic2 = ic * ic;
+    float a0 = (dp - rbar * c * dun) * 0.5f * ic2;
+    float a1 = drho - dp * ic2;
+    float a2 = rbar * dut;
+    float a3 = (dp + rbar * c * dun) * 0.5f * ic2;
+    float l0 = 0.5f * fabsf(un - c) * a0, l1 = 0.5f * fabsf(un) * a1;
+    float l2 = 0.5f * fabsf(un) * a2, l3 = 0.5f * fabsf(un + c) * a3;
+    float FL[4], FR[4];
+    pflux(L, FL);
+    pflux(R, FR);
+    F[0] = 0.5f * (FL[0] + FR[0]) - (l0 + l1 + l3);
+    F[1] = 0.5f * (FL[1] + FR[1]) - (l0 * (un - c) + l1 * un + l3 * (un + c));
+    F[2] = 0.5f * (FL[2] + FR[2]) - (l0 * ut + l1 * ut + l2 + l3 * ut);
+    F[3] = 0.5f * (FL[3] + FR[3]) -
+           (l0 * (H - un * c) + l1 * 0.5f * q2 + l2 * ut + l3 * (H + un * c));
+}
+
+// Local Lax-Friedrichs (include/scheme.h:229-381).
+__device__ __forceinline__ void llf(const Prim& L, const Prim& R, float gamma, float* F) {
+    float aL = sqr(gamma * L.p * L.ir), aR = sqr(gamma * R.p * R.ir);
+    float sp = fmaxf(fabsf(L.un) + aL, fabsf(R.un) + aR);
+    float FL[4], FR[4];
+    pflux(L, FL);
+    pflux(R, FR);
+    float UL[4] = {L.r, L.r * L.un, L.r * L.ut, L.E}, UR[4] = {R.r, R.r * R.un, R.r * R.ut, R.E};
+#pragma unroll
+    for (int k = 0; k < 4; k++) F[k] = 0.5f * (FL[k] + FR[k]) - 0.5f * sp * (UR[k] - UL[k]);
+}
+
+}  // namespace f32
+}  // namespace eb2

@@ -164,9 +164,12 @@ __global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
     // 3. interface fluxes: x faces (TX+1) x TY, then y faces TX x (TY+1)
     unsigned st = 0;
     const int pos = a.num.positivity;
+    // (faces that no interior cell of this tile uses -- past the domain edge in
+    // a partial tile -- are skipped)
     for (int job = threadIdx.x; job < NJX + NJY; job += NT) {
         if (job < NJX) {
             int rr = job / TY, cc = job - rr * TY;
+            if (i0 - 1 + rr >= rows - GC || j0 + cc >= cols - GC) continue;
             const double* s = sU + rr * HY + (cc + 3);
             const double* pa = sP + rr * PY + (cc + 1);
             st |= interface_flux<1, RECON, CHAR, WZ, FLUX>(s, HY, pa, pa + PY, a.grid.dx, g, pos,
@@ -174,6 +177,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
         } else {
             int q = job - NJX;
             int rr = q / (TY + 1), cc = q - rr * (TY + 1);
+            if (i0 + rr >= rows - GC || j0 - 1 + cc >= cols - GC) continue;
             const double* s = sU + (rr + 3) * HY + cc;
             const double* pa = sP + (rr + 1) * PY + cc;
             st |= interface_flux<2, RECON, CHAR, WZ, FLUX>(s, 1, pa, pa + 1, a.grid.dy, g, pos,

@@ -1,0 +1,286 @@
+// eb2_stage_mixed.cuh -- fused x+y sweep and SSP-RK stage, mixed precision.
+//
+// Same structure and contract as the FP64 form (eb2_stage_fp64.cuh): a CTA
+// stages a TX x TY tile plus 3-cell halo, computes every interface flux the
+// tile needs and applies flux difference + RK combination to its cells.
+// Differences: the staged tile is FP32, per-cell primitives come from FP64
+// arithmetic, interface work is FP32 in delta form (eb2_point_mixed.cuh), the
+// fluxes are widened to FP64 in shared memory, and the flux difference and
+// RK combination are FP64 with the stage input re-read in FP64.
+// Reconstruction: WENO5 in characteristic variables (Jiang-Shu or WENO-Z
+// weights).
+#pragma once
+
+#include "eb2_kernels.h"
+#include "eb2_point_mixed.cuh"
+
+namespace eb2 {
+namespace mixstage {
+
+constexpr int TX = 16, TY = 32, NT = 256;
+constexpr int HX = TX + 6, HY = TY + 6;
+constexpr int PX = TX + 2, PY = TY + 2;
+constexpr int FS = HX * HY;
+constexpr int PS = PX * PY;
+constexpr int XS = (TX + 1) * TY;
+constexpr int YS = TX * (TY + 1);
+constexpr int NJX = (TX + 1) * TY, NJY = TX * (TY + 1);
+// FP32 tile and primitives, FP64 interface fluxes (widened exactly once, so
+// that flux differences telescope and the step conserves to FP64 round-off)
+constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS) * sizeof(float) +
+                        (size_t)(4 * XS + 4 * YS) * sizeof(double);
+
+// One interface.  s: stencil cell n = 0 of field 0 (fields FS apart, `stride`
+// along the sweep); pa/pb: primitive records of cells i and i+1 (fields PS
+// apart); ga/gb: the two cells in global memory (near-vacuum path).
+template <int DIR, bool WZ, int FLUX>
+__device__ __forceinline__ unsigned interface_flux(const float* __restrict__ s, int stride,
+                                                   const float* __restrict__ pa,
+                                                   const float* __restrict__ pb,
+                                                   const double* __restrict__ u, size_t ga,
+                                                   size_t gb, size_t plane, float pthr,
+                                                   const Gas& g, int positivity,
+                                                   double* __restrict__ out, int ostride) {
+    const float gm1 = (float)g.gm1, gamma = (float)g.gamma;
+    f32::Eig e;
+    if (pa[f32::P_P * PS] < pthr || pb[f32::P_P * PS] < pthr) {
+        double qa[4], qb[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            qa[k] = u[ga + k * plane];
+            qb[k] = u[gb + k * plane];
+        }
+        e = f32::roe_f64(qa, qb, g.gm1, g.gr);
+    } else {
+        e = f32::roe_f32(pa, pb, PS, gm1);
+    }
+    const float b0 = s[2 * stride], b1 = s[FS + 2 * stride], b2 = s[2 * FS + 2 * stride],
+                b3 = s[3 * FS + 2 * stride];
+    float w[4][6];
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        if (n == 2) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) w[k][2] = 0.0f;
+            continue;
+        }
+        float d0 = s[n * stride] - b0, d1 = s[FS + n * stride] - b1;
+        float d2 = s[2 * FS + n * stride] - b2, d3 = s[3 * FS + n * stride] - b3;
+        float c[4];
+        f32::project<DIR>(e, d0, d1, d2, d3, c);
+#pragma unroll
+        for (int k = 0; k < 4; k++) w[k][n] = c[k];
+    }
+    float wm[4], wp[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        f32::weno5_pair<WZ>(w[k][0], w[k][1], w[k][3], w[k][4], w[k][5], wm[k], wp[k]);
+    float dqm[4], dqp[4];
+    f32::unproject<DIR>(e, wm, dqm);
+    f32::unproject<DIR>(e, wp, dqp);
+    const float rb = pa[f32::P_RHO * PS], ub = pa[f32::P_U * PS], vb = pa[f32::P_V * PS],
+                pbs = pa[f32::P_P * PS];
+    f32::Prim L = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, dqm, gm1);
+    f32::Prim R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, dqp, gm1);
+    unsigned st = 0;
+    if (!(L.r > 0.0f && L.p > 0.0f && R.r > 0.0f && R.p > 0.0f)) {
+        if (positivity) {
+            float z[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            float d[4] = {s[3 * stride] - b0, s[FS + 3 * stride] - b1,
+                          s[2 * FS + 3 * stride] - b2, s[3 * FS + 3 * stride] - b3};
+            L = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, z, gm1);
+            R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, d, gm1);
+        } else {
+            st |= ST_NONPHYSICAL;
+        }
+    }
+    float F[4];
+    if (FLUX == FLUX_HLLC) f32::hllc(L, R, gamma, F);
+    else if (FLUX == FLUX_ROE) f32::roe(L, R, gamma, F);
+    else if (FLUX == FLUX_HLL) f32::hll(L, R, gamma, F);
+    else f32::llf(L, R, gamma, F);
+    // (mass, normal, tangential, energy) -> (rho, rho u, rho v, rho E)
+    out[0] = (double)F[0];
+    out[ostride] = (double)(DIR == 1 ? F[1] : F[2]);
+    out[2 * ostride] = (double)(DIR == 1 ? F[2] : F[1]);
+    out[3 * ostride] = (double)F[3];
+    return st;
+}
+
+template <bool WZ, int FLUX>
+__global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
+    Ctrl* ctrl = a.ctrl;
+    if (!ctrl->active) return;
+    extern __shared__ double smd[];
+    double* sFx = smd;
+    double* sFy = sFx + 4 * XS;
+    float* sU = reinterpret_cast<float*>(sFy + 4 * YS);
+    float* sP = sU + 4 * FS;
+    __shared__ double red[3][NT / 32];
+
+    const int rows = a.grid.rows, cols = a.grid.cols;
+    const size_t plane = (size_t)rows * cols;
+    const int i0 = GC + blockIdx.y * TX, j0 = GC + blockIdx.x * TY;
+    const double* __restrict__ uin = a.uin;
+    const Gas g = a.gas;
+    const float pthr = (float)(1.0e-3 * ctrl->pmean);
+
+    // 1. tile + halo as FP32; primitives of the tile and its first ring from FP64
+    for (int e = threadIdx.x; e < FS; e += NT) {
+        int r = e / HY, c = e - r * HY;
+        int i = i0 - 3 + r, j = j0 - 3 + c;
+        double q[4] = {0.0, 0.0, 0.0, 0.0};
+        if (i < rows && j < cols) {
+            size_t o = (size_t)i * cols + j;
+#pragma unroll
+            for (int k = 0; k < 4; k++) q[k] = uin[o + k * plane];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) sU[k * FS + e] = (float)q[k];
+        int pr = r - 2, pc = c - 2;
+        if (pr >= 0 && pr < PX && pc >= 0 && pc < PY) {
+            double rho = q[0];
+            double ir = 1.0 / rho;
+            double uu = q[1] * ir, vv = q[2] * ir;
+            double p = (q[3] - 0.5 * (q[1] * uu + q[2] * vv)) * g.gm1;
+            int pe = pr * PY + pc;
+            sP[f32::P_RHO * PS + pe] = (float)rho;
+            sP[f32::P_U * PS + pe] = (float)uu;
+            sP[f32::P_V * PS + pe] = (float)vv;
+            sP[f32::P_P * PS + pe] = (float)p;
+            sP[f32::P_H * PS + pe] = (float)(g.gr * p * ir);
+            sP[f32::P_SR * PS + pe] = (float)sqrt(rho);
+        }
+    }
+    __syncthreads();
+
+    // 2. interface fluxes
+    unsigned st = 0;
+    const int pos = a.num.positivity;
+    for (int job = threadIdx.x; job < NJX + NJY; job += NT) {
+        if (job < NJX) {
+            int rr = job / TY, cc = job - rr * TY;
+            int i = i0 - 1 + rr, j = j0 + cc;
+            if (i >= rows - GC || j >= cols - GC) continue;  // past the domain edge
+            size_t ga = (size_t)i * cols + j;
+            const float* pa = sP + rr * PY + (cc + 1);
+            st |= interface_flux<1, WZ, FLUX>(sU + rr * HY + (cc + 3), HY, pa, pa + PY, uin, ga,
+                                              ga + cols, plane, pthr, g, pos, sFx + rr * TY + cc,
+                                              XS);
+        } else {
+            int q = job - NJX;
+            int rr = q / (TY + 1), cc = q - rr * (TY + 1);
+            int i = i0 + rr, j = j0 - 1 + cc;
+            if (i >= rows - GC || j >= cols - GC) continue;
+            size_t ga = (size_t)i * cols + j;
+            const float* pa = sP + (rr + 1) * PY + cc;
+            st |= interface_flux<2, WZ, FLUX>(sU + (rr + 3) * HY + cc, 1, pa, pa + 1, uin, ga,
+                                              ga + 1, plane, pthr, g, pos,
+                                              sFy + rr * (TY + 1) + cc, YS);
+        }
+    }
+    __syncthreads();
+
+    // 3. flux difference (widened to FP64), RK combination in FP64
+    const double dt = ctrl->dt;
+    const double idx = a.grid.inv_dx, idy = a.grid.inv_dy;
+    const double grav = a.num.gravity;
+    double mx = 0.0, my = 0.0, ps = 0.0;
+    for (int e = threadIdx.x; e < TX * TY; e += NT) {
+        int rr = e / TY, cc = e - rr * TY;
+        int i = i0 + rr, j = j0 + cc;
+        if (i >= rows - GC || j >= cols - GC) continue;
+        size_t o = (size_t)i * cols + j;
+        double x[4], src[4] = {0.0, 0.0, 0.0, 0.0}, out[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) x[k] = uin[o + k * plane];
+        if (a.num.source) {
+            double rho = x[0];
+            src[2] = rho * grav;
+            src[3] = rho * grav * (x[2] / rho);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double fxp = sFx[k * XS + (rr + 1) * TY + cc], fxm = sFx[k * XS + rr * TY + cc];
+            double fyp = sFy[k * YS + rr * (TY + 1) + cc + 1], fym = sFy[k * YS + rr * (TY + 1) + cc];
+            double L = -(fxp - fxm) * idx - (fyp - fym) * idy + src[k];
+            double y = a.combine == COMB_EULER ? x[k] : a.un[o + k * plane];
+            double r;
+            switch (a.combine) {
+                case COMB_EULER: r = y + dt * L; break;
+                case COMB_RK2: r = 0.5 * y + 0.5 * (x[k] + dt * L); break;
+                case COMB_RK3_2: r = 0.75 * y + 0.25 * (x[k] + dt * L); break;
+                default: r = (1.0 / 3.0) * y + (2.0 / 3.0) * (x[k] + dt * L); break;
+            }
+            out[k] = r;
+            a.uout[o + k * plane] = r;
+        }
+        if (isnan(out[0]) || isnan(out[3])) st |= ST_NAN_STATE;
+        if (a.partials) {
+            double rho = out[0];
+            double ir = 1.0 / rho;
+            double uu = out[1] * ir, vv = out[2] * ir;
+            double p = (out[3] - 0.5 * rho * (uu * uu + vv * vv)) * g.gm1;
+            double c = sqrt(g.gamma * p * ir);
+            double lx = fabs(uu) + c, ly = fabs(vv) + c;
+            if (lx > mx) mx = lx;
+            if (ly > my) my = ly;
+            ps += p;
+        }
+    }
+
+    unsigned wst = __reduce_or_sync(0xffffffffu, st);
+    if (wst && (threadIdx.x & 31) == 0) atomicOr(&ctrl->status, wst);
+    if (a.partials) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            double ox = __shfl_down_sync(0xffffffffu, mx, off);
+            double oy = __shfl_down_sync(0xffffffffu, my, off);
+            double op = __shfl_down_sync(0xffffffffu, ps, off);
+            if (ox > mx) mx = ox;
+            if (oy > my) my = oy;
+            ps += op;
+        }
+        int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) {
+            red[0][w] = mx;
+            red[1][w] = my;
+            red[2][w] = ps;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bx = 0.0, by = 0.0, bp = 0.0;
+            for (int q = 0; q < NT / 32; q++) {
+                if (red[0][q] > bx) bx = red[0][q];
+                if (red[1][q] > by) by = red[1][q];
+                bp += red[2][q];
+            }
+            size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+            a.partials[3 * b + 0] = bx;
+            a.partials[3 * b + 1] = by;
+            a.partials[3 * b + 2] = bp;
+        }
+    }
+}
+
+template <bool WZ, int FLUX>
+cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
+    auto kern = k_stage<WZ, FLUX>;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)SMEM);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    if (!a.uout) return cudaSuccess;
+    dim3 grid((a.grid.ny + TY - 1) / TY, (a.grid.nx + TX - 1) / TX);
+    kern<<<grid, NT, SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace mixstage
+}  // namespace eb2
