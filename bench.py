@@ -65,7 +65,115 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--serve", type=int, default=None, metavar="N",
+                    help="served stream of N requests only (batched vs one-at-a-time)")
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-baseline", type=int, default=24,
+                    help="requests of the stream timed one at a time in FP64")
+    ap.add_argument("--accuracy", type=float, default=None, metavar="T",
+                    help="run the FP64 and mixed forms to time T and print their difference")
     return ap.parse_args()
+
+
+def stream_trace(n, rate, seed, eb2):
+    """The served stream: n requests arriving Poisson at `rate` per second;
+    each a four-quadrant problem with per-quadrant rho ~ U[0.1,2],
+    p ~ U[0.05,2], u, v ~ U[-1.5,1.5] (positive by construction), or a
+    wall-heating problem with inflow speed ~ U[0.5,2] on the unit square
+    (periodic in y, so dx = dy); square grids from {128,256,512,1024}, final
+    time ~ U[0.1,0.3]."""
+    import numpy as np
+
+    from overheatingproblem_b200.server import Request
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    arrivals -= arrivals[0]
+    reqs = []
+    for _ in range(n):
+        size = int(rng.choice([128, 256, 512, 1024]))
+        tmax = float(rng.uniform(0.1, 0.3))
+        if rng.random() < 0.5:
+            q = []
+            for _ in range(4):
+                q += [rng.uniform(0.1, 2.0), rng.uniform(-1.5, 1.5), rng.uniform(-1.5, 1.5),
+                      rng.uniform(0.05, 2.0)]
+            reqs.append(Request(eb2.lib.CASE_FOUR_QUADRANT, size, size, q=q, tmax=tmax))
+        else:
+            reqs.append(Request(eb2.lib.CASE_WALL_HEATING, size, size,
+                                q=[float(rng.uniform(0.5, 2.0))], ly=1.0, tmax=tmax))
+    return reqs, arrivals
+
+
+def serve_stream(eb2, local, n, rate, seed, baseline_n):
+    """Batched mixed-precision server vs one-at-a-time plain FP64 solves on the
+    same trace: solves/s and latency percentiles (finish - arrival)."""
+    import numpy as np
+
+    from overheatingproblem_b200.server import Server
+    reqs, arr = stream_trace(n, rate, seed, eb2)
+    with Server(device=local, precision=eb2.lib.MIXED, scheme=2,
+                hbm_budget=120 * 10**9) as srv:
+        out = srv.run_trace(reqs, arr)
+    lat = out["finish"] - arr
+    batched = {"solves_per_s": n / out["makespan"], "makespan_s": out["makespan"],
+               "p50_latency_s": float(np.percentile(lat, 50)),
+               "p99_latency_s": float(np.percentile(lat, 99)), "requests": n}
+    # one-at-a-time plain FP64 launches: each request on its own context,
+    # started when it has arrived and the previous one has finished
+    m = min(baseline_n, n)
+    t0 = time.perf_counter()
+    fin = np.zeros(m)
+    for i in range(m):
+        wait = arr[i] - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        r = reqs[i]
+        with eb2.Solver(r.nx, r.ny, device=local, recon=5, characteristic=True, weno_z=False,
+                        cfl=r.cfl, precision=eb2.lib.FP64) as s:
+            lx, ly, _ = s.init_case(r.test_case, r.q)
+            ly = r.ly if r.ly > 0 else ly
+            s.run(ORDER, 2, lx / r.nx, ly / r.ny, r.tmax)
+            s.download()
+        fin[i] = time.perf_counter() - t0
+    blat = fin - arr[:m]
+    base = {"solves_per_s": m / fin[-1], "makespan_s": float(fin[-1]),
+            "p50_latency_s": float(np.percentile(blat, 50)),
+            "p99_latency_s": float(np.percentile(blat, 99)), "requests": m}
+    return {"trace": f"{n} requests, Poisson arrivals at {rate}/s, seed {seed}",
+            "batched_mixed": batched, "one_at_a_time_fp64": base,
+            "speedup_solves_per_s": batched["solves_per_s"] / base["solves_per_s"]}
+
+
+def run_accuracy(args, local):
+    """FP64 vs mixed on the benchmark problem to t = T: density/velocity/pressure
+    L1 (mean over cells) and Linf differences, steps and device-loop time."""
+    import numpy as np
+    import torch
+
+    import overheatingproblem_b200 as eb2
+
+    nx, scheme = args.nx, SCHEMES[args.scheme]
+    out, prim = {}, {}
+    for prec in ("fp64", "mixed"):
+        s = eb2.Solver(nx, nx, device=local, recon=5, characteristic=True, weno_z=False,
+                       cfl=0.5, precision=eb2.lib.FP64 if prec == "fp64" else eb2.lib.MIXED)
+        lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+        torch.cuda.synchronize(local)
+        t0 = time.perf_counter()
+        n, tf = s.run(ORDER, scheme, lx / nx, ly / nx, args.accuracy)
+        el = time.perf_counter() - t0
+        prim[prec] = s.con_to_pri()[:, 4:-4, 4:-4].copy()
+        out[prec] = {"steps": n, "t_final": tf, "seconds": el, "status_flags": s.status(),
+                     "cell_updates_per_s": nx * nx * n / el}
+        s.close()
+    d = np.abs(prim["fp64"] - prim["mixed"])
+    names = ["rho", "u", "v", "p"]
+    line = {"accuracy": workload(nx, "mixed", args.scheme) + f" vs FP64, t = {args.accuracy}",
+            "l1": {k: float(d[i].mean()) for i, k in enumerate(names)},
+            "linf": {k: float(d[i].max()) for i, k in enumerate(names)},
+            "rel_l1_rho": float(d[0].sum() / np.abs(prim["fp64"][0]).sum()),
+            "runs": out}
+    print(json.dumps(line), flush=True)
 
 
 def workload(nx, precision, scheme):
@@ -319,6 +427,9 @@ def run_ours(args, world, rank, local):
                           "ms_per_step": tot / k, "steps": k, "status_flags": st2,
                           "roofline_frac": n2 * n2 * BYTES_PER_CELL_STEP * k / (stm * 1e-3) / 1e9
                           / peak}
+        if rank == 0:
+            extra["served_stream"] = serve_stream(eb2, local, 24, args.serve_rate, 7,
+                                                  args.serve_baseline)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,7 +455,15 @@ def main():
     # the reference arm uses no collective: rank 0 works, the others leave
     world, rank, local = dist_setup(collective=args.impl == "ours")
     try:
-        if args.impl == "reference":
+        if args.accuracy is not None:
+            if rank == 0:
+                run_accuracy(args, local)
+        elif args.serve is not None:
+            if rank == 0:
+                import overheatingproblem_b200 as eb2
+                print(json.dumps(serve_stream(eb2, local, args.serve, args.serve_rate, 7,
+                                              args.serve_baseline)), flush=True)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

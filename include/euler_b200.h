@@ -38,7 +38,8 @@ enum {
     EB2_ENOMEM = 2,       /* device or host allocation failed                     */
     EB2_ECUDA = 3,        /* CUDA error, or no CUDA device (there is no CPU path) */
     EB2_ENONPHYS = 4,     /* non-physical state met (see eb2_status)              */
-    EB2_EUNSUPPORTED = 5  /* option the library does not implement               */
+    EB2_EUNSUPPORTED = 5, /* option the library does not implement               */
+    EB2_EBUSY = 6         /* server: no free slot or HBM budget for the request   */
 };
 
 /* Status bits accumulated by the kernels of a context. */
@@ -105,6 +106,9 @@ int eb2_set_positivity_fallback(eb2_ctx *ctx, int on);
 
 /* bc_config (include/Boundary_Condition.h:30-38). */
 int eb2_set_bc(eb2_ctx *ctx, int left, int right, int bottom, int top);
+/* The context's boundary kinds (left, right, bottom, top), e.g. as set by
+ * eb2_init_case the way Init_Euler_2D sets bc_config. */
+int eb2_get_bc(eb2_ctx *ctx, int *kinds4);
 /* inflow_state (Boundary_Condition.h:41,49) and L/R/B/T_fixed_value_state
  * (include/initialize.h:1298-1301), conserved variables; NULL keeps a value. */
 int eb2_set_bc_states(eb2_ctx *ctx, const double *inflow4, const double *fixed16);
@@ -118,6 +122,13 @@ int eb2_set_double_mach(eb2_ctx *ctx, int on);
  * returns its domain lengths and final time. */
 int eb2_init_case(eb2_ctx *ctx, int test_case, const double *q, double *lx, double *ly,
                   double *tmax);
+
+/* Init_Euler_2D in full: eb2_init_case, plus the case's primitive state
+ * (initEulerTestCase), and the physical fluxes of the initial state
+ * (initEulerflux2D, include/initialize.h:1409-1434) into host arrays
+ * pri, F, G [4][rows][cols]; any of them may be NULL. */
+int eb2_init_case_fields(eb2_ctx *ctx, int test_case, const double *q, double *pri,
+                         double *F, double *G, double *lx, double *ly, double *tmax);
 
 /* Copy the full state (ghosts included) between host and device. */
 int eb2_upload(eb2_ctx *ctx, const double *U);
@@ -157,10 +168,11 @@ int eb2_riemann(eb2_ctx *ctx, int scheme, int dir, const double *conserl,
 int eb2_flux_reconstruction(eb2_ctx *ctx, int scheme, double dx, double dy, double *f,
                             double *g);
 
-/* Space_Discrete_Item (include/scheme.h:3758-3777) with the gravity source of
- * the state (Source_Gravity, :3723) when Source is on. */
+/* Space_Discrete_Item (include/scheme.h:3758-3777): L = -(f_i - f_{i-1})/dx
+ * - (g_j - g_{j-1})/dy + s on the interior.  s == NULL takes the gravity
+ * source of the state (Source_Gravity, :3723) when Source is on, else zero. */
 int eb2_space_discrete(eb2_ctx *ctx, double dx, double dy, const double *f, const double *g,
-                       double *L);
+                       const double *s, double *L);
 
 /* Get_Delta_T_2D (include/function.h:144-175). */
 int eb2_delta_t(eb2_ctx *ctx, double dx, double dy, double *dt);
@@ -200,6 +212,55 @@ int eb2_advance(eb2_ctx *ctx, int order, int scheme, double dx, double dy, int n
 int eb2_bench_steps(eb2_ctx *ctx, int order, int scheme, double dx, double dy, int nsteps,
                     unsigned long long flush_bytes, float *step_ms, float *stage_ms,
                     int *stage_launches, long long *launches);
+
+/* --- solve server (no counterpart in the reference) -------------------------- */
+
+/* Many independent solves on one GPU with continuous batching.  Each request
+ * is one eb2_run-style solve (SSP-RK3, WENO5, CFL time step, its own final
+ * time) of an EB2_CASE_* initial state.  Admitted requests keep their state on
+ * the device and advance together: a batch step is one CUDA graph whose
+ * stage kernels walk a device work list of (solve, tile) pairs with a
+ * persistent grid (sized per batch shape by timing, the autotuner).  Requests
+ * are admitted while a slot is free and the HBM budget allows, and retired as
+ * they finish; a solve's result does not depend on what else is in the batch
+ * (the same bits as alone, and as eb2_run on a context). */
+typedef struct eb2_server eb2_server;
+
+typedef struct {
+    int test_case;        /* EB2_CASE_*                                         */
+    int nx, ny;           /* interior cells                                     */
+    int has_q;            /* q holds case parameters (see eb2_init_case)        */
+    double q[16];
+    double lx, ly;        /* domain lengths; <= 0 keeps the case's              */
+    double tmax;          /* final time; <= 0 keeps the case's                  */
+    double cfl;           /* CFL number; <= 0 gives 0.5                         */
+} eb2_request;
+
+/* scheme as AR_scheme; recon must be 5; the mixed form needs characteristic. */
+int eb2_server_create(eb2_server **out, int device, int max_slots,
+                      unsigned long long hbm_budget_bytes, int precision, int recon,
+                      int characteristic, int weno_z, int scheme, double gamma);
+int eb2_server_destroy(eb2_server *srv);
+/* Admit a request (EB2_EBUSY: no slot or budget now). */
+int eb2_server_submit(eb2_server *srv, const eb2_request *req, long long *id);
+/* Advance all admitted solves by `ngraphs` batch graphs (4 steps each); the
+ * number of solves that finished is returned in *nfinished. */
+int eb2_server_step(eb2_server *srv, int ngraphs, int *nfinished);
+/* Finished solves awaiting eb2_server_fetch: ids, final times, step counts. */
+int eb2_server_poll(eb2_server *srv, long long *ids, double *t_final, long long *steps,
+                    unsigned *status, int max, int *n);
+/* Copy a finished solve's state to U (may be NULL) and free its slot. */
+int eb2_server_fetch(eb2_server *srv, long long id, double *U);
+int eb2_server_stats(eb2_server *srv, unsigned long long *hbm_used, int *active,
+                     long long *graph_launches);
+/* The request loop: replay n requests arriving arrival_s[i] seconds after the
+ * call in real time (FIFO admission by slot and budget, batch steps, retire as
+ * finished).  Per request: admission and finish times in seconds since the
+ * start (either array may be NULL) and, when results != NULL and results[i]
+ * != NULL, the final state. */
+int eb2_server_run_trace(eb2_server *srv, const eb2_request *reqs, const double *arrival_s,
+                         int n, double *admit_s, double *finish_s, double **results,
+                         double *makespan_s);
 
 /* --- diagnostics ------------------------------------------------------------- */
 

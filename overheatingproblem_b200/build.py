@@ -35,11 +35,14 @@ CUDA_SOURCES = [
     ("eb2_stage.cu", True),
     ("eb2_aux.cu", True),
     ("eb2_api.cu", True),
+    ("eb2_batch_fp64.cu", True),
+    ("eb2_server.cu", True),
     ("eb2_stage_mixed.cu", False),
+    ("eb2_batch_mixed.cu", False),
 ]
 C_SOURCES = ["eb2_control.c"]
 HEADERS = ["eb2_common.cuh", "eb2_kernels.h", "eb2_point_fp64.cuh", "eb2_stage_fp64.cuh",
-           "eb2_point_mixed.cuh", "eb2_stage_mixed.cuh"]
+           "eb2_point_mixed.cuh", "eb2_stage_mixed.cuh", "eb2_loop.cuh", "eb2_batch.cuh"]
 
 
 def _nvcc() -> str:

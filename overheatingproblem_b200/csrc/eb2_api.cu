@@ -185,6 +185,13 @@ int read_status(eb2_ctx* c, unsigned* st) {
 }
 }  // namespace
 
+void eb2::set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+
+void eb2::set_loop_ctrl(Ctrl* c, double t0, double tmax, double out_dt, double cfl, double dmin,
+                        long long max_step, cudaStream_t s) {
+    k_set_loop<<<1, 1, 0, s>>>(c, t0, tmax, out_dt, cfl, dmin, max_step);
+}
+
 extern "C" {
 
 const char* eb2_last_error(void) { return g_err; }
@@ -325,6 +332,12 @@ int eb2_set_bc(eb2_ctx* c, int left, int right, int bottom, int top) {
     return EB2_OK;
 }
 
+int eb2_get_bc(eb2_ctx* c, int* kinds4) {
+    if (!c || !kinds4) return fail(EB2_EARG, "null argument");
+    for (int s = 0; s < 4; s++) kinds4[s] = c->bnd.kind[s];
+    return EB2_OK;
+}
+
 int eb2_set_bc_states(eb2_ctx* c, const double* inflow4, const double* fixed16) {
     if (!c) return fail(EB2_EARG, "null context");
     if (inflow4) memcpy(c->bnd.inflow, inflow4, sizeof c->bnd.inflow);
@@ -339,12 +352,15 @@ int eb2_set_double_mach(eb2_ctx* c, int on) {
     return EB2_OK;
 }
 
-int eb2_init_case(eb2_ctx* c, int tc, const double* q, double* lx, double* ly, double* tmax) {
-    if (int r = check(c)) return r;
-    InitDesc d;
+}  // extern "C"
+
+// Initial-state descriptor, domain lengths, final time and boundary kinds of
+// test case tc (shared by eb2_init_case and the solve server).
+int eb2::case_setup(int tc, const double* q, InitDesc& d, double* L, double& T, int* bc) {
     memset(&d, 0, sizeof d);
-    double L[2] = {1.0, 1.0}, T = 0.0;
-    int bc[4] = {BC_OUTFLOW, BC_OUTFLOW, BC_OUTFLOW, BC_OUTFLOW};
+    L[0] = L[1] = 1.0;
+    T = 0.0;
+    for (int s = 0; s < 4; s++) bc[s] = BC_OUTFLOW;
     auto put = [&](int s, double r, double u, double v, double p) {
         d.st[s][0] = r; d.st[s][1] = u; d.st[s][2] = v; d.st[s][3] = p;
     };
@@ -421,11 +437,44 @@ int eb2_init_case(eb2_ctx* c, int tc, const double* q, double* lx, double* ly, d
         default:
             return fail(EB2_EUNSUPPORTED, "test case %d is not implemented", tc);
     }
-    if (int r = eb2_set_bc(c, bc[0], bc[1], bc[2], bc[3])) return r;
-    c->bnd.dmr = 0;
     d.lx = L[0];
     d.ly = L[1];
+    return EB2_OK;
+}
+
+extern "C" {
+
+int eb2_init_case(eb2_ctx* c, int tc, const double* q, double* lx, double* ly, double* tmax) {
+    if (int r = check(c)) return r;
+    InitDesc d;
+    double L[2], T;
+    int bc[4];
+    if (int r = case_setup(tc, q, d, L, T, bc)) return r;
+    if (int r = eb2_set_bc(c, bc[0], bc[1], bc[2], bc[3])) return r;
+    c->bnd.dmr = 0;
     CK(launch_init(c->u, c->grid, c->gas, d, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (lx) *lx = L[0];
+    if (ly) *ly = L[1];
+    if (tmax) *tmax = T;
+    return EB2_OK;
+}
+
+int eb2_init_case_fields(eb2_ctx* c, int tc, const double* q, double* pri, double* F,
+                         double* G, double* lx, double* ly, double* tmax) {
+    if (int r = check(c)) return r;
+    InitDesc d;
+    double L[2], T;
+    int bc[4];
+    if (int r = case_setup(tc, q, d, L, T, bc)) return r;
+    if (int r = eb2_set_bc(c, bc[0], bc[1], bc[2], bc[3])) return r;
+    if (int r = ensure_tmp(c, 3)) return r;
+    c->bnd.dmr = 0;
+    CK(launch_init(c->u, c->grid, c->gas, d, c->stream, c->tmp[0], c->tmp[1], c->tmp[2]));
+    size_t b = c->nstate * sizeof(double);
+    double* out[3] = {pri, F, G};
+    for (int k = 0; k < 3; k++)
+        if (out[k]) CK(cudaMemcpyAsync(out[k], c->tmp[k], b, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (lx) *lx = L[0];
     if (ly) *ly = L[1];
@@ -554,16 +603,18 @@ int eb2_flux_reconstruction(eb2_ctx* c, int scheme, double dx, double dy, double
 }
 
 int eb2_space_discrete(eb2_ctx* c, double dx, double dy, const double* f, const double* g,
-                       double* L) {
+                       const double* s, double* L) {
     if (int r = check(c)) return r;
     if (!f || !g || !L) return fail(EB2_EARG, "null host array");
-    if (int r = ensure_tmp(c, 3)) return r;
+    if (int r = ensure_tmp(c, 4)) return r;
     set_spacing(c, dx, dy);
     size_t b = c->nstate * sizeof(double);
     CK(cudaMemcpyAsync(c->tmp[0], f, b, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->tmp[1], g, b, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->tmp[2], L, b, cudaMemcpyHostToDevice, c->stream));
-    CK(launch_space_item(c->tmp[0], c->tmp[1], c->u, c->tmp[2], c->grid, c->num, c->stream));
+    if (s) CK(cudaMemcpyAsync(c->tmp[3], s, b, cudaMemcpyHostToDevice, c->stream));
+    CK(launch_space_item(c->tmp[0], c->tmp[1], s ? c->tmp[3] : nullptr, c->u, c->tmp[2], c->grid,
+                         c->num, c->stream));
     CK(cudaMemcpyAsync(L, c->tmp[2], b, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return EB2_OK;

@@ -3,6 +3,7 @@
 // interface).  Built with -fmad=false: every value here must match the
 // reference's bits (see eb2_point_fp64.cuh).
 #include "eb2_kernels.h"
+#include "eb2_loop.cuh"
 #include "eb2_point_fp64.cuh"
 
 namespace eb2 {
@@ -16,95 +17,12 @@ inline int blocks_for(long long n, int nt = NT) {
 }
 }  // namespace
 
-// ---------------------------------------------------------------------------
-// Boundary_Conditions (include/Boundary_Condition.h:963-980) and
-// BC_DoubleMach_2D (:480-692).  One thread per ghost value of the four side
-// strips (4 layers x 4 fields x tangential extent).  Only non-corner ghosts
-// are written: no stencil, eigenvector or flux ever reads a corner ghost, and
-// with at least 4 interior cells behind a mirrored or periodic side every
-// source is an interior cell, so the four sides are independent and one
-// launch fills them all (the reference's L, R, B, T order only matters for
-// the corner cells).
-// ---------------------------------------------------------------------------
+// Ghost-cell fill (body in eb2_loop.cuh).
 __global__ void k_bc(double* __restrict__ u, Grid g, Boundary b, const Ctrl* ctrl,
                      double time) {
     if (ctrl && !ctrl->active) return;
-    const double t = ctrl ? ctrl->t : time;
-    const int rows = g.rows, cols = g.cols, nx = g.nx, ny = g.ny;
-    const long long nlr = 16LL * ny, nbt = 16LL * nx;
-    const long long total = 2 * nlr + 2 * nbt;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        int side;
-        long long q;
-        if (e < 2 * nlr) { side = (int)(e / nlr); q = e - side * nlr; }
-        else { long long f = e - 2 * nlr; side = 2 + (int)(f / nbt); q = f - (side - 2) * nbt; }
-        const int km = (int)(q & 15);
-        const int tpos = GC + (int)(q >> 4);    // tangential index (j for L/R, i for B/T)
-        const int k = km & 3, m = km >> 2;      // field, ghost layer (0 = next to the wall)
-        const bool lr = side < 2;
-        const int nlen = lr ? rows : cols;
-        const int ghost = (side == 0 || side == 2) ? GC - 1 - m : nlen - GC + m;
-        const int normal = lr ? 1 : 2;
-        int src = -1;
-        double cval = 0.0, sgn = 1.0;
-        if (b.dmr) {
-            // BC_DoubleMach_2D constants (Boundary_Condition.h:483-513)
-            const double gm = 1.4, x0 = 1.0 / 6.0;
-            const double post[4] = {8.0, 8.0 * 7.1447, 8.0 * -4.125,
-                                    116.5 / (gm - 1.0) + 0.5 * 8.0 * (7.1447 * 7.1447 + -4.125 * -4.125)};
-            const double pre[4] = {1.4, 1.4 * 0.0, 1.4 * 0.0,
-                                   1.0 / (gm - 1.0) + 0.5 * 1.4 * (0.0 * 0.0 + 0.0 * 0.0)};
-            const double xnx = rows - 2 * GC;
-            if (side == 0) {
-                cval = post[k];
-            } else if (side == 1) {
-                src = rows - GC - 1;
-            } else {
-                double xp = (double)(tpos + 0.5 - GC) / xnx * 4.0;
-                if (side == 2) {
-                    if (xp > x0) { src = GC + m; if (k == 2) sgn = -1.0; }
-                    else cval = post[k];
-                } else {
-                    double xs = x0 + (1.0 / sqrt(3.0)) + (20.0 * t / sqrt(3.0));
-                    cval = xp < xs ? post[k] : pre[k];
-                }
-            }
-        } else {
-            switch (b.kind[side]) {
-                case BC_OUTFLOW:
-                    src = (side == 0 || side == 2) ? GC : nlen - GC - 1;
-                    break;
-                case BC_PERIODIC:
-                    src = (side == 0 || side == 2) ? nlen - GC - 1 - m : GC + m;
-                    break;
-                case BC_REFLECT:
-                    // left and top mirror four layers (:356-374, :443-461); right
-                    // and bottom copy the wall cell (:393-407, :427-441)
-                    if (side == 0) src = GC + m;
-                    else if (side == 3) src = nlen - GC - 1 - m;
-                    else if (side == 1) src = nlen - GC - 1;
-                    else src = GC;
-                    if (k == normal) sgn = -1.0;
-                    break;
-                case BC_INFLOW:
-                    cval = b.inflow[k];
-                    break;
-                default:
-                    cval = b.fixed[side][k];
-                    break;
-            }
-        }
-        double val;
-        if (src >= 0) {
-            double sv = lr ? u[at(k, src, tpos, rows, cols)] : u[at(k, tpos, src, rows, cols)];
-            val = sgn < 0.0 ? -sv : sv;
-        } else {
-            val = cval;
-        }
-        if (lr) u[at(k, ghost, tpos, rows, cols)] = val;
-        else u[at(k, tpos, ghost, rows, cols)] = val;
-    }
+    bc_fill(u, g, b, ctrl ? ctrl->t : time, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+            (long long)gridDim.x * blockDim.x);
 }
 
 cudaError_t launch_bc(double* u, const Grid& g, const Boundary& b, const Ctrl* ctrl,
@@ -119,7 +37,8 @@ cudaError_t launch_bc(double* u, const Grid& g, const Boundary& b, const Ctrl* c
 // primitives, then initEulerconser2D (:1389-1405) converts the whole array.
 // ---------------------------------------------------------------------------
 __global__ void k_init(double* __restrict__ u, Grid g, Gas gas, InitDesc d,
-                       const double* __restrict__ column) {
+                       const double* __restrict__ column, double* __restrict__ pri,
+                       double* __restrict__ fx, double* __restrict__ gy) {
     const int rows = g.rows, cols = g.cols;
     const long long n = (long long)rows * cols;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
@@ -161,15 +80,29 @@ __global__ void k_init(double* __restrict__ u, Grid g, Gas gas, InitDesc d,
             w[0] = st[0]; w[1] = st[1]; w[2] = st[2]; w[3] = st[3];
         }
         double r = w[0], uu = w[1], vv = w[2], p = w[3];
-        u[at(0, i, j, rows, cols)] = r;
-        u[at(1, i, j, rows, cols)] = uu * r;
-        u[at(2, i, j, rows, cols)] = vv * r;
-        u[at(3, i, j, rows, cols)] = p / gas.gm1 + 0.5 * r * (uu * uu + vv * vv);
+        double q[4] = {r, uu * r, vv * r, p / gas.gm1 + 0.5 * r * (uu * uu + vv * vv)};
+        for (int k = 0; k < 4; k++) u[at(k, i, j, rows, cols)] = q[k];
+        if (pri)
+            for (int k = 0; k < 4; k++) pri[at(k, i, j, rows, cols)] = w[k];
+        if (fx) {
+            // initEulerflux2D (:1409-1434), from the conserved values (0/0 in
+            // cells the case leaves empty, as there)
+            double cu = q[1] / q[0], cv = q[2] / q[0];
+            double cp = (q[3] - 0.5 * r * (cu * cu + cv * cv)) * gas.gm1;
+            fx[at(0, i, j, rows, cols)] = r * cu;
+            fx[at(1, i, j, rows, cols)] = r * cu * cu + cp;
+            fx[at(2, i, j, rows, cols)] = r * cu * cv;
+            fx[at(3, i, j, rows, cols)] = (q[3] + cp) * cu;
+            gy[at(0, i, j, rows, cols)] = r * cv;
+            gy[at(1, i, j, rows, cols)] = r * cu * cv;
+            gy[at(2, i, j, rows, cols)] = r * cv * cv + cp;
+            gy[at(3, i, j, rows, cols)] = (q[3] + cp) * cv;
+        }
     }
 }
 
 cudaError_t launch_init(double* u, const Grid& g, const Gas& gas, const InitDesc& d,
-                        cudaStream_t s) {
+                        cudaStream_t s, double* pri, double* fx, double* gy) {
     const double* column = nullptr;
     double* dcol = nullptr;
     if (d.kind == INIT_SINE) {
@@ -188,7 +121,7 @@ cudaError_t launch_init(double* u, const Grid& g, const Gas& gas, const InitDesc
         column = dcol;
     }
     long long n = (long long)g.rows * g.cols;
-    k_init<<<blocks_for(n), NT, 0, s>>>(u, g, gas, d, column);
+    k_init<<<blocks_for(n), NT, 0, s>>>(u, g, gas, d, column, pri, fx, gy);
     cudaError_t e = cudaGetLastError();
     if (dcol) cudaFreeAsync(dcol, s);
     return e;
@@ -199,36 +132,6 @@ cudaError_t launch_init(double* u, const Grid& g, const Gas& gas, const InitDesc
 // independent; the pressure sum (used by the mixed form's near-vacuum test)
 // is reduced in a fixed order, so both are deterministic.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void block_reduce3(double& mx, double& my, double& ps, double* red) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        double ox = __shfl_down_sync(0xffffffffu, mx, off);
-        double oy = __shfl_down_sync(0xffffffffu, my, off);
-        double op = __shfl_down_sync(0xffffffffu, ps, off);
-        if (ox > mx) mx = ox;
-        if (oy > my) my = oy;
-        ps += op;
-    }
-    int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        red[w] = mx;
-        red[32 + w] = my;
-        red[64 + w] = ps;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double bx = 0.0, by = 0.0, bp = 0.0;
-        for (int q = 0; q < nw; q++) {
-            if (red[q] > bx) bx = red[q];
-            if (red[32 + q] > by) by = red[32 + q];
-            bp += red[64 + q];
-        }
-        mx = bx;
-        my = by;
-        ps = bp;
-    }
-}
-
 __global__ void k_wave_partials(const double* __restrict__ u, Grid g, Gas gas,
                                 double* __restrict__ partials) {
     __shared__ double red[96];
@@ -266,47 +169,11 @@ cudaError_t launch_wave_partials(const double* u, const Grid& g, const Gas& gas,
     return cudaGetLastError();
 }
 
-// Reduce the partials and advance the device copy of the host time loop of
-// src/RP_FVM.c:179-267.
+// End-of-step reduction and time bookkeeping (body in eb2_loop.cuh).
 __global__ void k_finalize(Ctrl* c, const double* __restrict__ partials, int nblocks,
                            int ncells, int mode) {
     __shared__ double red[96];
-    if (mode == 2 && !c->active) return;
-    double mx = 0.0, my = 0.0, ps = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-        double a0 = partials[3 * b], a1 = partials[3 * b + 1];
-        if (a0 > mx) mx = a0;
-        if (a1 > my) my = a1;
-        ps += partials[3 * b + 2];
-    }
-    block_reduce3(mx, my, ps, red);
-    if (threadIdx.x != 0) return;
-    c->sx = mx;
-    c->sy = my;
-    c->pmean = ps / ncells;
-    // dt = CFL * min(dx, dy) / (max|u|+a + max|v|+a)
-    double dt = c->cfl * c->dmin / (mx + my);
-    if (mode == 0) {
-        c->dt = dt;
-        return;
-    }
-    if (mode == 2) {
-        double now = c->t + c->dt;
-        if (fabs(now - c->next_out) < 1e-10 * c->out_dt) {
-            c->out_pending = 1;
-            c->next_out += c->out_dt;
-        }
-        c->t = now;
-        c->step += 1;
-    }
-    if (c->t + dt > c->next_out) dt = c->next_out - c->t;
-    if (c->t + dt >= c->tmax) dt = c->tmax - c->t;
-    c->dt = dt;
-    if (!(dt > 0.0) || isinf(dt)) {
-        if (c->t < c->tmax) c->status |= ST_BAD_DT;
-    }
-    c->active = (c->t < c->tmax) && !c->out_pending && !(c->status & ST_BAD_DT) &&
-                c->step < c->max_step;
+    finalize_body(c, partials, nblocks, ncells, mode, red);
 }
 
 cudaError_t launch_finalize(Ctrl* ctrl, const double* partials, int nblocks, int ncells,
@@ -560,15 +427,17 @@ cudaError_t launch_riemann(int dir, const double* ql, const double* qr, double* 
 // Space_Discrete_Item (include/scheme.h:3758-3777) with the gravity source of
 // Source_Gravity (:3723-3751) taken from u when n.source is set.
 __global__ void k_space_item(const double* __restrict__ f, const double* __restrict__ gf,
-                             const double* __restrict__ u, double* __restrict__ lout, Grid g,
-                             Numerics nm) {
+                             const double* __restrict__ s, const double* __restrict__ u,
+                             double* __restrict__ lout, Grid g, Numerics nm) {
     const int rows = g.rows, cols = g.cols;
     const long long n = (long long)g.nx * g.ny;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x) {
         int i = GC + (int)(e / g.ny), j = GC + (int)(e % g.ny);
         double src[4] = {0.0, 0.0, 0.0, 0.0};
-        if (nm.source) {
+        if (s) {
+            for (int k = 0; k < 4; k++) src[k] = s[at(k, i, j, rows, cols)];
+        } else if (nm.source) {
             double rho = u[at(0, i, j, rows, cols)];
             double v = u[at(2, i, j, rows, cols)] / rho;
             src[2] = rho * nm.gravity;
@@ -582,9 +451,10 @@ __global__ void k_space_item(const double* __restrict__ f, const double* __restr
     }
 }
 
-cudaError_t launch_space_item(const double* f, const double* gflux, const double* u,
-                              double* lout, const Grid& g, const Numerics& n, cudaStream_t s) {
-    k_space_item<<<blocks_for((long long)g.nx * g.ny), NT, 0, s>>>(f, gflux, u, lout, g, n);
+cudaError_t launch_space_item(const double* f, const double* gflux, const double* src,
+                              const double* u, double* lout, const Grid& g, const Numerics& n,
+                              cudaStream_t s) {
+    k_space_item<<<blocks_for((long long)g.nx * g.ny), NT, 0, s>>>(f, gflux, src, u, lout, g, n);
     return cudaGetLastError();
 }
 

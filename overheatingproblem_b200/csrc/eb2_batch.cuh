@@ -1,0 +1,68 @@
+// eb2_batch.cuh -- batched kernels of the solve server: many independent
+// solves of different sizes advanced together, each with its own time step.
+//
+// Every solve ("slot") has a descriptor in device memory.  A device-resident
+// work list holds one (slot, tile) pair per tile of every active slot; the
+// stage kernels run a persistent grid whose CTAs walk that list, so one launch
+// advances a stage of all slots and small solves share the GPU with large ones.
+// Boundary fill and the end-of-step reduction run one block row per slot.
+// The per-tile work is the single-solve kernels' own stage_tile, so a slot
+// evolves bit for bit as the same solve run alone.
+#pragma once
+
+#include "eb2_kernels.h"
+
+namespace eb2 {
+
+struct SlotDesc {
+    double* u;            // state
+    double* u1;           // stage 1 output
+    double* u2;           // stage 2 output
+    double* partials;     // wave-speed partials, one triple per tile
+    Ctrl* ctrl;           // control block of this solve
+    Grid grid;
+    Gas gas;
+    Numerics num;
+    Boundary bnd;
+    int tiles_x;          // tiles along y
+    int ntiles;
+    int ncells;
+};
+
+// Stage buffers of SSP-RK3 (the server runs third-order steps only).
+__device__ __forceinline__ void rk3_buffers(const SlotDesc& s, int stage, const double*& in,
+                                            double*& out, int& comb) {
+    if (stage == 0) { in = s.u; out = s.u1; comb = COMB_EULER; }
+    else if (stage == 1) { in = s.u1; out = s.u2; comb = COMB_RK3_2; }
+    else { in = s.u2; out = s.u; comb = COMB_RK3_3; }
+}
+
+__device__ __forceinline__ StageArgs slot_args(const SlotDesc& s, int stage) {
+    StageArgs a;
+    rk3_buffers(s, stage, a.uin, a.uout, a.combine);
+    a.un = s.u;
+    a.grid = s.grid;
+    a.gas = s.gas;
+    a.num = s.num;
+    a.ctrl = s.ctrl;
+    a.partials = stage == 2 ? s.partials : nullptr;
+    return a;
+}
+
+// Host-side launch interface (eb2_batch_fp64.cu / eb2_batch_mixed.cu).
+struct BatchLaunch {
+    const SlotDesc* slots;   // device array of nslots descriptors
+    int nslots;
+    const int2* work;        // device work list: (slot, tile)
+    const int* nwork;        // device: number of work items
+    int grid;                // persistent CTAs of the stage kernels
+};
+cudaError_t launch_stage_batch_fp64(const BatchLaunch& b, const Numerics& num, int stage,
+                                    cudaStream_t s);
+cudaError_t launch_stage_batch_mixed(const BatchLaunch& b, const Numerics& num, int stage,
+                                     cudaStream_t s);
+cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s);
+cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s);
+int stage_batch_max_blocks_per_sm(int precision);
+
+}  // namespace eb2

@@ -9,7 +9,12 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
+
+// Point arithmetic is host-and-device so that it can also be exercised on the
+// CPU (eb2_pointcheck.cu).
+#define EB2_HD __host__ __device__ __forceinline__
 
 namespace eb2 {
 

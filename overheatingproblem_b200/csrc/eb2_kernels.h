@@ -27,6 +27,9 @@ struct StageArgs {
     double* partials;     // per-block {max|u|+a, max|v|+a, sum p} of uout, or null
 };
 
+// Message returned by eb2_last_error() for the calling thread (not exported).
+void set_last_error(const char* msg);
+
 // Fused x+y sweep + RK combine, FP64 bit-parity form.
 cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s);
 // Same contract, mixed precision (FP32 reconstruction and fluxes).
@@ -60,7 +63,8 @@ cudaError_t launch_recon(int dir, const double* u, double* ql, double* qr, const
 cudaError_t launch_riemann(int dir, const double* ql, const double* qr, double* f,
                            const Grid& g, const Gas& gas, int flux, unsigned* status,
                            cudaStream_t s);
-cudaError_t launch_space_item(const double* f, const double* gflux, const double* u,
+cudaError_t launch_space_item(const double* f, const double* gflux, const double* src,
+                              const double* u,
                               double* lout, const Grid& g, const Numerics& n, cudaStream_t s);
 
 // Initial states.
@@ -71,7 +75,18 @@ struct InitDesc {
     double lx, ly;
 };
 enum : int { INIT_UNIFORM = 0, INIT_HALF_X = 1, INIT_QUADRANT = 2, INIT_DMR = 3, INIT_SINE = 4 };
+
+// Initial state, domain lengths L[2], final time and boundary kinds bc[4] of
+// an EB2_CASE_* test case (eb2_api.cu).  Returns EB2_OK or an EB2_E* code.
+int case_setup(int tc, const double* q, InitDesc& d, double* L, double& T, int* bc);
+
+// Context-free pieces of the device loop (eb2_api.cu).
+void set_loop_ctrl(Ctrl* c, double t0, double tmax, double out_dt, double cfl, double dmin,
+                   long long max_step, cudaStream_t s);
+// Writes the conserved state; pri (the case's primitives) and the initial
+// physical fluxes fx, gy (initEulerflux2D) too when not null.
 cudaError_t launch_init(double* u, const Grid& g, const Gas& gas, const InitDesc& d,
-                        cudaStream_t s);
+                        cudaStream_t s, double* pri = nullptr, double* fx = nullptr,
+                        double* gy = nullptr);
 
 }  // namespace eb2

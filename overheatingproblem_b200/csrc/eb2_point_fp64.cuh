@@ -19,7 +19,7 @@ struct Roe {
 };
 
 // a = (rho, u, v, p, H) of the left cell, b of the right cell.
-__device__ __forceinline__ Roe roe_average(const double* a, const double* b, double gm1) {
+EB2_HD Roe roe_average(const double* a, const double* b, double gm1) {
     Roe r;
     double D = sqrt(b[0] / a[0]);
     double D1 = D + 1.0;
@@ -40,7 +40,7 @@ __device__ __forceinline__ Roe roe_average(const double* a, const double* b, dou
 // Row k of the left-eigenvector matrix (eigen_l[k][*], Characteriz.h:346-367
 // for x, :448-469 for y).
 template <int DIR>
-__device__ __forceinline__ void left_row(const Roe& e, int k, double* l) {
+EB2_HD void left_row(const Roe& e, int k, double* l) {
     if (DIR == 1) {
         switch (k) {
             case 0: l[0] = 0.5 * (e.b2 + e.uc); l[1] = -0.5 * (e.b1 * e.u + e.ic);
@@ -65,7 +65,7 @@ __device__ __forceinline__ void left_row(const Roe& e, int k, double* l) {
 // Row m of the right-eigenvector matrix, R[m][k] = eigen_r[m][k]
 // (Characteriz.h:371-392 for x, :473-494 for y).
 template <int DIR>
-__device__ __forceinline__ void right_row(const Roe& e, int m, double* r) {
+EB2_HD void right_row(const Roe& e, int m, double* r) {
     if (DIR == 1) {
         switch (m) {
             case 0: r[0] = 1.0; r[1] = e.b1; r[2] = 0.0; r[3] = 1.0; break;
@@ -84,7 +84,7 @@ __device__ __forceinline__ void right_row(const Roe& e, int m, double* r) {
 }
 
 // Jiang-Shu smoothness indicators (include/Reconstruction.h:1425-1432).
-__device__ __forceinline__ void smooth3(double v1, double v2, double v3, double v4, double v5,
+EB2_HD void smooth3(double v1, double v2, double v3, double v4, double v5,
                                         double& s1, double& s2, double& s3) {
     s1 = 13.0 / 12.0 * (v1 - 2.0 * v2 + v3) * (v1 - 2.0 * v2 + v3)
        + 0.25 * (v1 - 4.0 * v2 + 3.0 * v3) * (v1 - 4.0 * v2 + 3.0 * v3);
@@ -95,7 +95,7 @@ __device__ __forceinline__ void smooth3(double v1, double v2, double v3, double 
 }
 
 // Nonlinear blend of the three candidate stencils (Reconstruction.h:1440-1454).
-__device__ __forceinline__ double blend3(double a1, double a2, double a3, double v1, double v2,
+EB2_HD double blend3(double a1, double a2, double a3, double v1, double v2,
                                          double v3, double v4, double v5) {
     double w1 = a1 / (a1 + a2 + a3);
     double w2 = a2 / (a1 + a2 + a3);
@@ -107,7 +107,7 @@ __device__ __forceinline__ double blend3(double a1, double a2, double a3, double
 
 // WENO5_L with Jiang-Shu weights (Reconstruction.h:1408-1455); WENO5_R is the
 // same function on the mirrored stencil.
-__device__ __forceinline__ double weno5_js(double v1, double v2, double v3, double v4, double v5) {
+EB2_HD double weno5_js(double v1, double v2, double v3, double v4, double v5) {
     const double eps = 1.0e-15;
     double s1, s2, s3;
     smooth3(v1, v2, v3, v4, v5, s1, s2, s3);
@@ -118,7 +118,7 @@ __device__ __forceinline__ double weno5_js(double v1, double v2, double v3, doub
 }
 
 // WENO5Z_L / WENO5Z_R (Reconstruction.h:1519-1624).
-__device__ __forceinline__ double weno5_z(double v1, double v2, double v3, double v4, double v5) {
+EB2_HD double weno5_z(double v1, double v2, double v3, double v4, double v5) {
     const double eps = 1.0e-15;
     double s1, s2, s3;
     smooth3(v1, v2, v3, v4, v5, s1, s2, s3);
@@ -129,13 +129,13 @@ __device__ __forceinline__ double weno5_z(double v1, double v2, double v3, doubl
     return blend3(a1, a2, a3, v1, v2, v3, v4, v5);
 }
 
-__device__ __forceinline__ int sgn(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+EB2_HD int sgn(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
 
 // TVD_minmod_* / TVD_vanleer_* (Reconstruction.h:1088-1201) with the limiters
 // min_mod and van_leer of include/function.h:66-74.  side +1 returns the value
 // at the right face of cell c, side -1 at its left face.
 template <bool VANLEER>
-__device__ __forceinline__ double muscl(double lo, double c, double hi, double delta, int side) {
+EB2_HD double muscl(double lo, double c, double hi, double delta, int side) {
     double s1 = (c - lo) / delta;
     double s2 = (hi - c) / delta;
     double s;
@@ -152,7 +152,7 @@ __device__ __forceinline__ double muscl(double lo, double c, double hi, double d
 // Interface pair (minus side, plus side) from six values q[0..5] = cells
 // i-2..i+3 of one field; RECON 5 = WENO5, 2 = TVD, 1 = first order.
 template <int RECON, bool WZ, bool VANLEER>
-__device__ __forceinline__ void recon_pair(const double* q, double delta, double& qm, double& qp) {
+EB2_HD void recon_pair(const double* q, double delta, double& qm, double& qp) {
     if (RECON == 5) {
         if (WZ) {
             qm = weno5_z(q[0], q[1], q[2], q[3], q[4]);
@@ -175,7 +175,7 @@ struct Side {
     double r, ru, rv, re, ir, u, v, uu, vv, p;
 };
 
-__device__ __forceinline__ Side unpack(const double* q, double gm1) {
+EB2_HD Side unpack(const double* q, double gm1) {
     Side s;
     s.r = q[0]; s.ru = q[1]; s.rv = q[2]; s.re = q[3];
     s.ir = 1.0 / s.r;
@@ -189,7 +189,7 @@ __device__ __forceinline__ Side unpack(const double* q, double gm1) {
 
 // Physical flux along DIR with total enthalpy H.
 template <int DIR>
-__device__ __forceinline__ void phys_flux(const Side& s, double H, double* F) {
+EB2_HD void phys_flux(const Side& s, double H, double* F) {
     if (DIR == 1) {
         F[0] = s.r * s.u;
         F[1] = s.r * s.uu + s.p;
@@ -206,7 +206,7 @@ __device__ __forceinline__ void phys_flux(const Side& s, double H, double* F) {
 // HLLC_Flux (include/scheme.h:690-1001).  The x sweep takes the sound speed
 // from the enthalpy (:745-746), the y sweep from gamma*p/rho (:895-896).
 template <int DIR>
-__device__ __forceinline__ void flux_hllc(const double* ql, const double* qr, const Gas& g,
+EB2_HD void flux_hllc(const double* ql, const double* qr, const Gas& g,
                                           double* F) {
     Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
     double HL, HR, aL, aR;
@@ -276,7 +276,7 @@ __device__ __forceinline__ void flux_hllc(const double* ql, const double* qr, co
 // skips the interface (`continue` on rho<=0, NaN rho, or NaN wave speed,
 // :427-436 and :500-503) and leaves its flux entry untouched.
 template <int DIR>
-__device__ __forceinline__ bool flux_hll(const double* ql, const double* qr, const Gas& g,
+EB2_HD bool flux_hll(const double* ql, const double* qr, const Gas& g,
                                          double* F) {
     if (ql[0] <= 0.0 || qr[0] <= 0.0) return false;
     if (isnan(ql[0]) || isnan(qr[0])) return false;
@@ -316,7 +316,7 @@ __device__ __forceinline__ bool flux_hll(const double* ql, const double* qr, con
 // Roe_Flux (include/scheme.h:1018-1322); its entropy fix is a no-op
 // (:1117-1126), so |lambda| is used directly.
 template <int DIR>
-__device__ __forceinline__ void flux_roe(const double* ql, const double* qr, const Gas& g,
+EB2_HD void flux_roe(const double* ql, const double* qr, const Gas& g,
                                          double* F) {
     Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
     double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
@@ -367,7 +367,7 @@ __device__ __forceinline__ void flux_roe(const double* ql, const double* qr, con
 
 // LLF_Flux (include/scheme.h:229-381), the dispatch default.
 template <int DIR>
-__device__ __forceinline__ void flux_llf(const double* ql, const double* qr, const Gas& g,
+EB2_HD void flux_llf(const double* ql, const double* qr, const Gas& g,
                                          double* F) {
     Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
     double aL = sqrt(g.gamma * L.p * L.ir), aR = sqrt(g.gamma * R.p * R.ir);
@@ -386,7 +386,7 @@ __device__ __forceinline__ void flux_llf(const double* ql, const double* qr, con
 
 // Riemann dispatch.  Returns false when HLL skipped the interface.
 template <int FLUX, int DIR>
-__device__ __forceinline__ bool riemann(const double* ql, const double* qr, const Gas& g,
+EB2_HD bool riemann(const double* ql, const double* qr, const Gas& g,
                                         double* F) {
     if (FLUX == FLUX_HLL) return flux_hll<DIR>(ql, qr, g, F);
     if (FLUX == FLUX_HLLC) flux_hllc<DIR>(ql, qr, g, F);
@@ -398,7 +398,7 @@ __device__ __forceinline__ bool riemann(const double* ql, const double* qr, cons
 // Primitive state of one cell plus its enthalpy: Con_to_Pri_2D
 // (include/initialize.h:1443-1446) and the H of Compute_Eigen_2DX
 // (include/Characteriz.h:319).
-__device__ __forceinline__ void primitive5(double r, double ru, double rv, double re,
+EB2_HD void primitive5(double r, double ru, double rv, double re,
                                            const Gas& g, double* w) {
     double u = ru / r;
     double v = rv / r;
@@ -411,7 +411,7 @@ __device__ __forceinline__ void primitive5(double r, double ru, double rv, doubl
 }
 
 // Is a reconstructed conserved state admissible (rho > 0, p > 0, finite)?
-__device__ __forceinline__ bool admissible(const double* q, double gm1) {
+EB2_HD bool admissible(const double* q, double gm1) {
     double r = q[0];
     if (!(r > 0.0)) return false;
     double u = q[1] / r, v = q[2] / r;

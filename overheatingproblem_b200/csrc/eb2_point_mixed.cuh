@@ -14,11 +14,13 @@
 //    H - q^2/2, b2 = b1 q^2 / 2, and interface pressures are p_base +
 //    (gamma-1)(dE - dK) with dK the kinetic-energy change written in
 //    differences; cell pressures themselves come from FP64;
-//  * rescaled epsilon -- the WENO weights are formed with one reciprocal per
+//  * rescaled weights -- the WENO weights are formed with one reciprocal per
 //    side from products of (beta + eps)^2 after scaling the stencil by a power
-//    of two; the reference's absolute eps = 1e-15 (Reconstruction.h:1414)
-//    becomes a relative floor eps = 1e-6 * s^2, s the stencil's largest
-//    difference, above FP32 rounding noise.
+//    of two and the (beta + eps) by the power of two of the smallest; eps is
+//    the reference's absolute 1e-15 (Reconstruction.h:1414) carried into the
+//    scaled units.  Where FP32 rounding noise in beta exceeds eps the
+//    candidate values agree to that noise, so the weights it picks do not
+//    show in the result.
 // Interfaces next to near-vacuum cells (p < 1e-3 of the mean pressure) get
 // their Roe eigenvectors from FP64 arithmetic.
 #pragma once
@@ -28,20 +30,63 @@
 namespace eb2 {
 namespace f32 {
 
-__device__ __forceinline__ float rcp(float x) {
+// Approximate reciprocal / reciprocal square root: the SFU instructions on the
+// GPU, plain IEEE arithmetic on the host (CPU checks of this file).
+EB2_HD float rcp(float x) {
+#ifdef __CUDA_ARCH__
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
+#else
+    return 1.0f / x;
+#endif
 }
-__device__ __forceinline__ float rsq(float x) {
+EB2_HD float rsq(float x) {
+#ifdef __CUDA_ARCH__
     float r;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
+#else
+    return 1.0f / sqrtf(x);
+#endif
 }
-__device__ __forceinline__ float sqr(float x) { return x * rsq(x); }  // sqrt for x > 0
+EB2_HD int bits_of(float x) {
+#ifdef __CUDA_ARCH__
+    return __float_as_int(x);
+#else
+    int i;
+    memcpy(&i, &x, sizeof i);
+    return i;
+#endif
+}
+EB2_HD float float_of(int i) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(i);
+#else
+    float x;
+    memcpy(&x, &i, sizeof x);
+    return x;
+#endif
+}
+EB2_HD float sqr(float x) { return x * rsq(x); }  // sqrt for x > 0
 
 // Per-cell primitive data kept in shared memory (FP32 values of FP64 results).
 enum : int { P_RHO = 0, P_U = 1, P_V = 2, P_P = 3, P_H = 4, P_SR = 5, NP = 6 };
+
+// Primitive record of one cell from its FP64 conserved state: the pressure is
+// formed in FP64 (E - kinetic cancels in low-pressure flows), then stored FP32.
+EB2_HD void cell_prims(const double* q, const Gas& g, float* P, int ps) {
+    double rho = q[0];
+    double ir = 1.0 / rho;
+    double uu = q[1] * ir, vv = q[2] * ir;
+    double p = (q[3] - 0.5 * (q[1] * uu + q[2] * vv)) * g.gm1;
+    P[P_RHO * ps] = (float)rho;
+    P[P_U * ps] = (float)uu;
+    P[P_V * ps] = (float)vv;
+    P[P_P * ps] = (float)p;
+    P[P_H * ps] = (float)(g.gr * p * ir);
+    P[P_SR * ps] = (float)sqrt(rho);
+}
 
 // Eigen-system parameters at an interface (the Roe average), in the form the
 // factored projections below use.
@@ -49,7 +94,7 @@ struct Eig {
     float u, v, c, hb1, hic, hq2, cg, b1, H;
 };
 
-__device__ __forceinline__ Eig eig_from(float u, float v, float c2, float gm1) {
+EB2_HD Eig eig_from(float u, float v, float c2, float gm1) {
     Eig e;
     float ic = rsq(c2);
     e.u = u;
@@ -68,7 +113,7 @@ __device__ __forceinline__ Eig eig_from(float u, float v, float c2, float gm1) {
 
 // Roe average from FP32 cell data: weights sqrt(rho), sound speed from the
 // cell enthalpies h (no H - q^2/2 cancellation).
-__device__ __forceinline__ Eig roe_f32(const float* a, const float* b, int ps, float gm1) {
+EB2_HD Eig roe_f32(const float* a, const float* b, int ps, float gm1) {
     float sa = a[P_SR * ps], sb = b[P_SR * ps];
     float rs = rcp(sa + sb);
     float wa = sa * rs, wb = sb * rs;
@@ -83,7 +128,7 @@ __device__ __forceinline__ Eig roe_f32(const float* a, const float* b, int ps, f
 
 // The same average in FP64 from the cells' FP64 conserved states (near-vacuum
 // interfaces): the reference's own formulas (Characteriz.h:333-342).
-__device__ __forceinline__ Eig roe_f64(const double* qa, const double* qb, double gm1,
+EB2_HD Eig roe_f64(const double* qa, const double* qb, double gm1,
                                        double gr) {
     double ua = qa[1] / qa[0], va = qa[2] / qa[0];
     double ub = qb[1] / qb[0], vb = qb[2] / qb[0];
@@ -112,7 +157,7 @@ __device__ __forceinline__ Eig roe_f64(const double* qa, const double* qb, doubl
 // Characteristic variables of a conserved difference d (left-eigenvector rows
 // of Characteriz.h:346-367 / :448-469 in factored form).
 template <int DIR>
-__device__ __forceinline__ void project(const Eig& e, float d0, float d1, float d2, float d3,
+EB2_HD void project(const Eig& e, float d0, float d1, float d2, float d3,
                                         float* w) {
     float K = fmaf(e.hq2, d0, d3);
     K = fmaf(-e.u, d1, K);
@@ -128,7 +173,7 @@ __device__ __forceinline__ void project(const Eig& e, float d0, float d1, float 
 // Conserved difference from characteristic values (right eigenvectors,
 // Characteriz.h:371-392 / :473-494, factored).
 template <int DIR>
-__device__ __forceinline__ void unproject(const Eig& e, const float* w, float* q) {
+EB2_HD void unproject(const Eig& e, const float* w, float* q) {
     float S = fmaf(e.b1, w[1], w[0] + w[3]);
     float D = w[0] - w[3];
     float cD = e.c * D;
@@ -146,21 +191,36 @@ __device__ __forceinline__ void unproject(const Eig& e, const float* w, float* q
 
 // WENO5 at both sides of an interface from the six characteristic values
 // w[0..5] (cells i-2..i+3) with w[2] == 0 (delta form around cell i).
-// Returns the minus-side value (WENO5_L on i-2..i+2) and the plus-side value
-// (WENO5_R on i+3..i-1).  WZ selects WENO-Z weights.
+// Returns the minus-side value (WENO5_L on i-2..i+2) relative to cell i and
+// the plus-side value (WENO5_R on i+3..i-1) relative to cell i+1 (minus w3),
+// so that a flat upwind side returns its own cell's state exactly, as the
+// FP64 form does.  WZ selects WENO-Z weights.
 template <bool WZ>
-__device__ __forceinline__ void weno5_pair(float w0, float w1, float w3, float w4, float w5,
+EB2_HD void weno5_pair(float w0, float w1, float w3, float w4, float w5,
                                            float& qm, float& qp) {
-    // power-of-two scale of the stencil, so that the products below stay in range
+    // scale the stencil by the power of two 2^-e of its largest magnitude
+    // s = m 2^e (exact), so that every value lies in (-2, 2) and the products
+    // of (beta + eps)^2 below stay inside the FP32 range
     float s = fmaxf(fmaxf(fmaxf(fabsf(w0), fabsf(w1)), fmaxf(fabsf(w3), fabsf(w4))), fabsf(w5));
-    if (!(s > 0.0f)) {  // flat (or non-finite) stencil
-        qm = qp = (s == 0.0f) ? 0.0f : s;
+    int ex = (bits_of(s) >> 23) & 0xff;
+    if (!(s > 0.0f) || ex == 0xff || ex < 2) {  // flat, non-finite or denormal stencil
+        qm = qp = (s == 0.0f || ex < 2) ? 0.0f : s;
         return;
     }
-    // 2^-e with s = m * 2^e, m in [1, 2): exact scaling
-    float sc = __int_as_float((254 - ((__float_as_int(s) >> 23) & 0xff)) << 23);
-    float sc2 = sc * sc;
-    const float k13 = 13.0f / 12.0f, eps = 1.0e-6f;
+    const float sc = float_of((254 - ex) << 23), inv_sc = float_of(ex << 23);
+    w0 *= sc;
+    w1 *= sc;
+    w3 *= sc;
+    w4 *= sc;
+    w5 *= sc;
+    const float k13 = 13.0f / 12.0f;
+    // The reference's absolute epsilon (1e-15 on the unscaled smoothness
+    // indicators, Reconstruction.h WENO5-JS/Z) in the scaled units: 1e-15 sc^2,
+    // clamped to the normal FP32 range.  Above the clamp beta / eps is below FP32
+    // resolution (linear weights either way); below it eps only matters for a
+    // beta that is exactly zero.
+    const int e2 = min(max(2 * (127 - ex), -75), 100);
+    const float eps = 1.0e-15f * float_of((127 + e2) << 23);
     // second differences shared by both sides
     float a1 = fmaf(-2.0f, w1, w0);          // w0 - 2 w1 + w2
     float a2 = w1 + w3;                      // w1 - 2 w2 + w3
@@ -177,13 +237,25 @@ __device__ __forceinline__ void weno5_pair(float w0, float w1, float w3, float w
     float bL3 = fmaf(0.25f * bl3, bl3, A3);
     float bR1 = fmaf(0.25f * br1, br1, A4), bR2 = fmaf(0.25f * br2, br2, A3);
     float bR3 = fmaf(0.25f * br3, br3, A2);
-    // candidate stencil values times 6 (Reconstruction.h:1452-1454 with w2 = 0)
-    float cl1 = fmaf(2.0f, w0, -7.0f * w1);
-    float c2 = fmaf(2.0f, w3, -w1);          // left candidate 2 == right candidate 3
-    float c3 = fmaf(5.0f, w3, -w4);          // left candidate 3 == right candidate 2
-    float cr1 = fmaf(2.0f, w5, fmaf(-7.0f, w4, 11.0f * w3));
+    // candidate stencil values times 6 (Reconstruction.h:1452-1454), minus
+    // 6 w2 = 0 on the left and minus 6 w3 on the right
+    float cl1 = fmaf(2.0f, w0, -7.0f * w1);  // stencil i-2..i
+    float c2 = fmaf(2.0f, w3, -w1);          // stencil i-1..i+1
+    float c3 = fmaf(5.0f, w3, -w4);          // stencil i..i+2
+    const float r1 = w1 - w3, r2 = -w3, r4 = w4 - w3, r5 = w5 - w3;
+    float cr1 = fmaf(2.0f, r5, -7.0f * r4);  // stencil i+1..i+3
+    float cr2 = fmaf(2.0f, r2, -r4);         // stencil i..i+2
+    float cr3 = fmaf(5.0f, r2, -r1);         // stencil i-1..i+1
     auto side = [&](float b1, float b2, float b3, float k1, float k2, float k3) {
-        float t1 = fmaf(b1, sc2, eps), t2 = fmaf(b2, sc2, eps), t3 = fmaf(b3, sc2, eps);
+        float t1 = b1 + eps, t2 = b2 + eps, t3 = b3 + eps;
+        // The weights are ratios: divide by the power of two of the smallest t
+        // (which lands in [1, 2)) and cap the others at 2^30, past which their
+        // weight is below FP32 resolution, so no product below leaves the range.
+        const float tm = fminf(fminf(t1, t2), t3);
+        const float nrm = float_of((254 - (int)((bits_of(tm) >> 23) & 0xff)) << 23);
+        t1 = fminf(t1 * nrm, 1073741824.0f);
+        t2 = fminf(t2 * nrm, 1073741824.0f);
+        t3 = fminf(t3 * nrm, 1073741824.0f);
         float g1, g2, g3;
         if (WZ) {
             // WENO-Z (Reconstruction.h:1546-1551): a_k = d_k (1 + tau5 / (beta_k + eps))
@@ -201,8 +273,8 @@ __device__ __forceinline__ void weno5_pair(float w0, float w1, float w3, float w
         float r = rcp(g1 + g2 + g3) * (1.0f / 6.0f);
         return fmaf(g1, k1, fmaf(g2, k2, g3 * k3)) * r;
     };
-    qm = side(bL1, bL2, bL3, cl1, c2, c3);
-    qp = side(bR1, bR2, bR3, cr1, c3, c2);
+    qm = side(bL1, bL2, bL3, cl1, c2, c3) * inv_sc;
+    qp = side(bR1, bR2, bR3, cr1, cr2, cr3) * inv_sc;
 }
 
 // Interface state in primitive form from the base cell and a conserved
@@ -212,7 +284,7 @@ struct Prim {
 };
 
 template <int DIR>
-__device__ __forceinline__ Prim prim_from_delta(float rb, float ub, float vb, float pb, float Eb,
+EB2_HD Prim prim_from_delta(float rb, float ub, float vb, float pb, float Eb,
                                                 const float* dq, float gm1) {
     Prim s;
     float r = rb + dq[0];
@@ -234,7 +306,7 @@ __device__ __forceinline__ Prim prim_from_delta(float rb, float ub, float vb, fl
 }
 
 // Physical flux in (mass, normal momentum, tangential momentum, energy) order.
-__device__ __forceinline__ void pflux(const Prim& s, float* F) {
+EB2_HD void pflux(const Prim& s, float* F) {
     float m = s.r * s.un;
     F[0] = m;
     F[1] = fmaf(m, s.un, s.p);
@@ -244,7 +316,7 @@ __device__ __forceinline__ void pflux(const Prim& s, float* F) {
 
 // HLLC with Einfeldt speeds (include/scheme.h:690-1001, sound speed
 // sqrt(gamma p / rho) on both sweeps).
-__device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float gamma, float* F) {
+EB2_HD void hllc(const Prim& L, const Prim& R, float gamma, float* F) {
     float aL2 = gamma * L.p * L.ir, aR2 = gamma * R.p * R.ir;
     float sqL = sqr(L.r), sqR = sqr(R.r);
     float is = rcp(sqL + sqR);
@@ -278,7 +350,7 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float gamma, 
 }
 
 // HLL with Einfeldt speeds (include/scheme.h:400-674).
-__device__ __forceinline__ void hll(const Prim& L, const Prim& R, float gamma, float* F) {
+EB2_HD void hll(const Prim& L, const Prim& R, float gamma, float* F) {
     float aL2 = gamma * L.p * L.ir, aR2 = gamma * R.p * R.ir;
     float sqL = sqr(L.r), sqR = sqr(R.r);
     float is = rcp(sqL + sqR);
@@ -299,7 +371,7 @@ __device__ __forceinline__ void hll(const Prim& L, const Prim& R, float gamma, f
 }
 
 // Roe flux with |lambda| (include/scheme.h:1018-1322), normal-aligned.
-__device__ __forceinline__ void roe(const Prim& L, const Prim& R, float gamma, float* F) {
+EB2_HD void roe(const Prim& L, const Prim& R, float gamma, float* F) {
     float gm1 = gamma - 1.0f;
     float sqL = sqr(L.r), sqR = sqr(R.r);
     float is = rcp(sqL + sqR);
@@ -331,7 +403,7 @@ __device__ __forceinline__ void roe(const Prim& L, const Prim& R, float gamma, f
 }
 
 // Local Lax-Friedrichs (include/scheme.h:229-381).
-__device__ __forceinline__ void llf(const Prim& L, const Prim& R, float gamma, float* F) {
+EB2_HD void llf(const Prim& L, const Prim& R, float gamma, float* F) {
     float aL = sqr(gamma * L.p * L.ir), aR = sqr(gamma * R.p * R.ir);
     float sp = fmaxf(fabsf(L.un) + aL, fabsf(R.un) + aR);
     float FL[4], FR[4];

@@ -1,0 +1,546 @@
+// eb2_server.cu -- the solve server: continuous batching of independent
+// solves on one GPU (include/euler_b200.h, eb2_server_*).
+//
+// Requests are admitted into slots while the HBM budget allows; each slot
+// keeps its state, stage buffers, partials and control block on the device
+// until it is retired.  All active slots advance together: one batch step is a
+// CUDA graph of seven launches (boundary fill + fused stage, three times, and
+// the per-slot end-of-step reduction) whose stage kernels walk the device
+// work list of (slot, tile) pairs with a persistent grid.  Admission and
+// retirement only rewrite the work list and descriptor arrays, so the graphs
+// are reused; a graph is captured per persistent-grid size, and the size is
+// picked per batch-shape class by timing the candidates (the autotuner).
+// Every slot has its own time, CFL step and final time.
+#include <algorithm>
+#include <cstdarg>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "../../include/euler_b200.h"
+#include "eb2_batch.cuh"
+
+using namespace eb2;
+
+namespace {
+
+constexpr int kStepsPerGraph = 4;
+
+struct Slot {
+    bool used = false;
+    bool done = false;
+    long long id = -1;
+    size_t bytes = 0;
+    double* u = nullptr;
+    double* u1 = nullptr;
+    double* u2 = nullptr;
+    double* partials = nullptr;
+    int nx = 0, ny = 0;
+    double t_final = 0.0;
+    long long steps = 0;
+    unsigned status = 0;
+};
+
+int fail(int code, const char* fmt, ...) {
+    char buf[256];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    set_last_error(buf);
+    return code;
+}
+
+#define CKS(expr)                                                                        \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(EB2_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_));             \
+    } while (0)
+
+size_t slot_bytes(int nx, int ny) {
+    size_t n = (size_t)4 * (nx + 2 * GC) * (ny + 2 * GC) * sizeof(double);
+    int tiles = std::max(((ny + 31) / 32) * ((nx + 15) / 16), 296);
+    return 3 * n + (size_t)3 * tiles * sizeof(double);
+}
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+struct eb2_server {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int precision = EB2_MIXED;
+    Numerics num{};
+    double gamma = 1.4;
+    size_t budget = 0, used = 0;
+    int nslots = 0;
+    std::vector<Slot> slots;
+    SlotDesc* d_desc = nullptr;
+    SlotDesc* h_desc = nullptr;   // pinned
+    Ctrl* d_ctrl = nullptr;
+    Ctrl* h_ctrl = nullptr;       // pinned
+    int2* d_work = nullptr;
+    int2* h_work = nullptr;       // pinned
+    int* d_nwork = nullptr;
+    int* h_nwork = nullptr;       // pinned
+    int work_cap = 0;
+    int nwork = 0;
+    bool dirty = true;
+    long long next_id = 0;
+    int sms = 148;
+    std::map<int, cudaGraphExec_t> graphs;   // persistent grid -> graph
+    std::map<int, int> tuned;                // shape class -> persistent grid
+    long long graph_launches = 0;
+};
+
+namespace {
+
+void destroy_graphs(eb2_server* s) {
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+}
+
+cudaError_t stage_batch(eb2_server* s, const BatchLaunch& b, int stage) {
+    return s->precision == EB2_MIXED ? launch_stage_batch_mixed(b, s->num, stage, s->stream)
+                                     : launch_stage_batch_fp64(b, s->num, stage, s->stream);
+}
+
+int get_graph(eb2_server* s, int grid, cudaGraphExec_t* out) {
+    auto it = s->graphs.find(grid);
+    if (it != s->graphs.end()) {
+        *out = it->second;
+        return EB2_OK;
+    }
+    BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0};
+    CKS(stage_batch(s, b, 0));  // kernel attributes, outside the capture
+    b.grid = grid;
+    cudaGraph_t g = nullptr;
+    CKS(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < kStepsPerGraph && !e; k++) {
+        for (int st = 0; st < 3 && !e; st++) {
+            e = launch_bc_batch(b, st, s->stream);
+            if (!e) e = stage_batch(s, b, st);
+        }
+        if (!e) e = launch_finalize_batch(b, s->stream);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+    if (e || e2) {
+        if (g) cudaGraphDestroy(g);
+        return fail(EB2_ECUDA, "batch graph capture: %s", cudaGetErrorString(e ? e : e2));
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e) return fail(EB2_ECUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+    s->graphs[grid] = ex;
+    *out = ex;
+    return EB2_OK;
+}
+
+// Rewrite the work list and descriptors after admissions and retirements.
+int rebuild(eb2_server* s) {
+    int n = 0;
+    for (int q = 0; q < s->nslots; q++)
+        if (s->slots[q].used && !s->slots[q].done) n += s->h_desc[q].ntiles;
+    if (n > s->work_cap) {
+        int cap = std::max(n, 2 * s->work_cap);
+        if (s->d_work) CKS(cudaFreeAsync(s->d_work, s->stream));
+        if (s->h_work) {
+            CKS(cudaStreamSynchronize(s->stream));
+            cudaFreeHost(s->h_work);
+        }
+        CKS(cudaMallocAsync(&s->d_work, (size_t)cap * sizeof(int2), s->stream));
+        CKS(cudaMallocHost(&s->h_work, (size_t)cap * sizeof(int2)));
+        s->work_cap = cap;
+        destroy_graphs(s);  // graphs hold the old work-list address
+    }
+    CKS(cudaStreamSynchronize(s->stream));  // the pinned staging arrays are reused
+    int w = 0;
+    for (int q = 0; q < s->nslots; q++) {
+        if (!s->slots[q].used || s->slots[q].done) continue;
+        for (int t = 0; t < s->h_desc[q].ntiles; t++) s->h_work[w++] = make_int2(q, t);
+    }
+    *s->h_nwork = w;
+    s->nwork = w;
+    if (w) CKS(cudaMemcpyAsync(s->d_work, s->h_work, (size_t)w * sizeof(int2),
+                               cudaMemcpyHostToDevice, s->stream));
+    CKS(cudaMemcpyAsync(s->d_nwork, s->h_nwork, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    CKS(cudaMemcpyAsync(s->d_desc, s->h_desc, (size_t)s->nslots * sizeof(SlotDesc),
+                        cudaMemcpyHostToDevice, s->stream));
+    s->dirty = false;
+    return EB2_OK;
+}
+
+int shape_class(int nwork) {
+    int c = 0;
+    while ((1 << c) < nwork) c++;
+    return c;
+}
+
+// One graph launch (kStepsPerGraph batch steps) with the tuned persistent grid.
+int launch_steps(eb2_server* s) {
+    const int maxb = stage_batch_max_blocks_per_sm(s->precision == EB2_MIXED ? 1 : 0);
+    const int cls = shape_class(s->nwork);
+    auto it = s->tuned.find(cls);
+    if (it == s->tuned.end()) {
+        // autotune: time each persistent-grid candidate on this batch; the
+        // slots advance during the trials, which is ordinary progress
+        int best = 0;
+        float best_ms = 1e30f;
+        cudaEvent_t e0, e1;
+        CKS(cudaEventCreate(&e0));
+        CKS(cudaEventCreate(&e1));
+        for (int mult = 1; mult <= maxb; mult++) {
+            int grid = std::min(mult * s->sms, std::max(s->nwork, 1));
+            cudaGraphExec_t ex;
+            if (int r = get_graph(s, grid, &ex)) return r;
+            CKS(cudaEventRecord(e0, s->stream));
+            CKS(cudaGraphLaunch(ex, s->stream));
+            CKS(cudaEventRecord(e1, s->stream));
+            CKS(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            s->graph_launches++;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = grid;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        s->tuned[cls] = best;
+        return EB2_OK;
+    }
+    cudaGraphExec_t ex;
+    if (int r = get_graph(s, it->second, &ex)) return r;
+    CKS(cudaGraphLaunch(ex, s->stream));
+    s->graph_launches++;
+    return EB2_OK;
+}
+
+// Read every slot's control block; mark the finished ones.
+int harvest(eb2_server* s, int* nfinished) {
+    CKS(cudaMemcpyAsync(s->h_ctrl, s->d_ctrl, (size_t)s->nslots * sizeof(Ctrl),
+                        cudaMemcpyDeviceToHost, s->stream));
+    CKS(cudaStreamSynchronize(s->stream));
+    int n = 0;
+    for (int q = 0; q < s->nslots; q++) {
+        Slot& sl = s->slots[q];
+        if (!sl.used || sl.done) continue;
+        const Ctrl& c = s->h_ctrl[q];
+        if (!c.active) {
+            sl.done = true;
+            sl.t_final = c.t;
+            sl.steps = c.step;
+            sl.status = c.status;
+            s->dirty = true;
+            n++;
+        }
+    }
+    if (nfinished) *nfinished = n;
+    return EB2_OK;
+}
+
+int find_slot(eb2_server* s, long long id) {
+    for (int q = 0; q < s->nslots; q++)
+        if (s->slots[q].used && s->slots[q].id == id) return q;
+    return -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int eb2_server_create(eb2_server** out, int device, int max_slots,
+                      unsigned long long hbm_budget_bytes, int precision, int recon,
+                      int characteristic, int weno_z, int scheme, double gamma) {
+    if (!out) return fail(EB2_EARG, "null output");
+    *out = nullptr;
+    if (max_slots < 1 || max_slots > 65535) return fail(EB2_EARG, "max_slots out of range");
+    if (precision != EB2_FP64 && precision != EB2_MIXED) return fail(EB2_EARG, "precision");
+    if (recon != 5) return fail(EB2_EUNSUPPORTED, "the server runs WENO5 reconstructions");
+    if (precision == EB2_MIXED && !characteristic)
+        return fail(EB2_EUNSUPPORTED, "the mixed form reconstructs in characteristic variables");
+    if (scheme == 11 || scheme == 22 || scheme == 33)
+        return fail(EB2_EUNSUPPORTED, "heat-conduction schemes are not implemented");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(EB2_ECUDA, "no CUDA device available; there is no CPU path");
+    if (device < 0 || device >= ndev) return fail(EB2_EARG, "device out of range");
+    CKS(cudaSetDevice(device));
+    eb2_server* s = new (std::nothrow) eb2_server();
+    if (!s) return fail(EB2_ENOMEM, "host allocation failed");
+    s->device = device;
+    s->precision = precision;
+    s->num.recon = recon;
+    s->num.characteristic = characteristic ? 1 : 0;
+    s->num.weno_z = weno_z ? 1 : 0;
+    s->num.flux = scheme == 1 ? FLUX_HLL : scheme == 2 ? FLUX_HLLC : scheme == 3 ? FLUX_ROE : FLUX_LLF;
+    s->gamma = gamma;
+    s->budget = hbm_budget_bytes;
+    s->nslots = max_slots;
+    s->slots.resize(max_slots);
+    cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
+    auto bail = [&](int code) {
+        eb2_server_destroy(s);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) ||
+        cudaMalloc(&s->d_desc, (size_t)max_slots * sizeof(SlotDesc)) ||
+        cudaMallocHost(&s->h_desc, (size_t)max_slots * sizeof(SlotDesc)) ||
+        cudaMalloc(&s->d_ctrl, (size_t)max_slots * sizeof(Ctrl)) ||
+        cudaMallocHost(&s->h_ctrl, (size_t)max_slots * sizeof(Ctrl)) ||
+        cudaMalloc(&s->d_nwork, sizeof(int)) || cudaMallocHost(&s->h_nwork, sizeof(int)))
+        return bail(fail(EB2_ENOMEM, "server allocation failed"));
+    memset(s->h_desc, 0, (size_t)max_slots * sizeof(SlotDesc));
+    if (cudaMemsetAsync(s->d_ctrl, 0, (size_t)max_slots * sizeof(Ctrl), s->stream) ||
+        cudaMemcpyAsync(s->d_desc, s->h_desc, (size_t)max_slots * sizeof(SlotDesc),
+                        cudaMemcpyHostToDevice, s->stream) ||
+        cudaStreamSynchronize(s->stream))
+        return bail(fail(EB2_ECUDA, "server initialisation failed"));
+    *out = s;
+    return EB2_OK;
+}
+
+int eb2_server_destroy(eb2_server* s) {
+    if (!s) return EB2_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    destroy_graphs(s);
+    for (auto& sl : s->slots)
+        if (sl.used) {
+            cudaFree(sl.u);
+            cudaFree(sl.u1);
+            cudaFree(sl.u2);
+            cudaFree(sl.partials);
+        }
+    cudaFree(s->d_desc);
+    cudaFreeHost(s->h_desc);
+    cudaFree(s->d_ctrl);
+    cudaFreeHost(s->h_ctrl);
+    cudaFree(s->d_work);
+    cudaFreeHost(s->h_work);
+    cudaFree(s->d_nwork);
+    cudaFreeHost(s->h_nwork);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return EB2_OK;
+}
+
+int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
+    if (!s || !r) return fail(EB2_EARG, "null argument");
+    if (r->nx < 1 || r->ny < 1) return fail(EB2_EARG, "empty grid");
+    CKS(cudaSetDevice(s->device));
+    InitDesc d;
+    double L[2], T;
+    int bc[4];
+    if (int rc = case_setup(r->test_case, r->has_q ? r->q : nullptr, d, L, T, bc)) return rc;
+    if (r->lx > 0.0) L[0] = d.lx = r->lx;
+    if (r->ly > 0.0) L[1] = d.ly = r->ly;
+    if (r->tmax > 0.0) T = r->tmax;
+    for (int q = 0; q < 4; q++) {
+        int n = q < 2 ? r->nx : r->ny;
+        if ((bc[q] == BC_PERIODIC || (bc[q] == BC_REFLECT && (q == 0 || q == 3))) && n < GC)
+            return fail(EB2_EUNSUPPORTED, "mirrored or periodic side needs 4 interior cells");
+    }
+    const size_t bytes = slot_bytes(r->nx, r->ny);
+    if (s->used + bytes > s->budget) return fail(EB2_EBUSY, "HBM budget exhausted");
+    int q = -1;
+    for (int k = 0; k < s->nslots; k++)
+        if (!s->slots[k].used) {
+            q = k;
+            break;
+        }
+    if (q < 0) return fail(EB2_EBUSY, "no free slot");
+    Slot& sl = s->slots[q];
+    const int rows = r->nx + 2 * GC, cols = r->ny + 2 * GC;
+    const size_t n = (size_t)4 * rows * cols * sizeof(double);
+    const int ntiles = ((r->ny + 31) / 32) * ((r->nx + 15) / 16);
+    const int npart = std::max(ntiles, 296);
+    CKS(cudaMallocAsync(&sl.u, n, s->stream));
+    CKS(cudaMallocAsync(&sl.u1, n, s->stream));
+    CKS(cudaMallocAsync(&sl.u2, n, s->stream));
+    CKS(cudaMallocAsync(&sl.partials, (size_t)3 * npart * sizeof(double), s->stream));
+    CKS(cudaMemsetAsync(sl.u, 0, n, s->stream));
+    CKS(cudaMemsetAsync(sl.u1, 0, n, s->stream));
+    CKS(cudaMemsetAsync(sl.u2, 0, n, s->stream));
+    SlotDesc& sd = s->h_desc[q];
+    memset(&sd, 0, sizeof sd);
+    sd.u = sl.u;
+    sd.u1 = sl.u1;
+    sd.u2 = sl.u2;
+    sd.partials = sl.partials;
+    sd.ctrl = s->d_ctrl + q;
+    sd.grid.nx = r->nx;
+    sd.grid.ny = r->ny;
+    sd.grid.rows = rows;
+    sd.grid.cols = cols;
+    sd.grid.dx = L[0] / r->nx;
+    sd.grid.dy = L[1] / r->ny;
+    sd.grid.inv_dx = 1.0 / sd.grid.dx;
+    sd.grid.inv_dy = 1.0 / sd.grid.dy;
+    sd.gas = Gas{s->gamma, s->gamma - 1.0, s->gamma / (s->gamma - 1.0)};
+    sd.num = s->num;
+    const double mach3[4] = {1.4, 1.4 * 3.0, 0.0, 1.0 / 0.4 + 0.5 * 1.4 * 3.0 * 3.0};
+    for (int k = 0; k < 4; k++) {
+        sd.bnd.kind[k] = bc[k];
+        sd.bnd.inflow[k] = mach3[k];
+        for (int m = 0; m < 4; m++) sd.bnd.fixed[m][k] = mach3[k];
+    }
+    sd.tiles_x = (r->ny + 31) / 32;
+    sd.ntiles = ntiles;
+    sd.ncells = r->nx * r->ny;
+    CKS(launch_init(sl.u, sd.grid, sd.gas, d, s->stream));
+    // control block and first CFL step, as eb2_run starts a solve
+    const double cfl = r->cfl > 0.0 ? r->cfl : 0.5;
+    const double dmin = sd.grid.dx > sd.grid.dy ? sd.grid.dy : sd.grid.dx;
+    CKS(cudaMemsetAsync(s->d_ctrl + q, 0, sizeof(Ctrl), s->stream));
+    set_loop_ctrl(s->d_ctrl + q, 0.0, T, T, cfl, dmin, LLONG_MAX, s->stream);
+    int nb = 0;
+    CKS(launch_wave_partials(sl.u, sd.grid, sd.gas, sl.partials, &nb, s->stream));
+    CKS(launch_finalize(s->d_ctrl + q, sl.partials, nb, sd.ncells, 1, s->stream));
+    sl.used = true;
+    sl.done = false;
+    sl.id = s->next_id++;
+    sl.bytes = bytes;
+    sl.nx = r->nx;
+    sl.ny = r->ny;
+    s->used += bytes;
+    s->dirty = true;
+    if (id) *id = sl.id;
+    return EB2_OK;
+}
+
+int eb2_server_step(eb2_server* s, int ngraphs, int* nfinished) {
+    if (!s) return fail(EB2_EARG, "null server");
+    CKS(cudaSetDevice(s->device));
+    if (s->dirty)
+        if (int r = rebuild(s)) return r;
+    if (nfinished) *nfinished = 0;
+    if (s->nwork == 0) return EB2_OK;
+    for (int k = 0; k < ngraphs; k++)
+        if (int r = launch_steps(s)) return r;
+    return harvest(s, nfinished);
+}
+
+int eb2_server_poll(eb2_server* s, long long* ids, double* t_final, long long* steps,
+                    unsigned* status, int max, int* n) {
+    if (!s || !n) return fail(EB2_EARG, "null argument");
+    int k = 0;
+    for (int q = 0; q < s->nslots && k < max; q++) {
+        const Slot& sl = s->slots[q];
+        if (!sl.used || !sl.done) continue;
+        if (ids) ids[k] = sl.id;
+        if (t_final) t_final[k] = sl.t_final;
+        if (steps) steps[k] = sl.steps;
+        if (status) status[k] = sl.status;
+        k++;
+    }
+    *n = k;
+    return EB2_OK;
+}
+
+int eb2_server_fetch(eb2_server* s, long long id, double* U) {
+    if (!s) return fail(EB2_EARG, "null server");
+    CKS(cudaSetDevice(s->device));
+    int q = find_slot(s, id);
+    if (q < 0) return fail(EB2_EARG, "unknown request id %lld", id);
+    Slot& sl = s->slots[q];
+    if (!sl.done) return fail(EB2_EBUSY, "request %lld has not finished", id);
+    if (U) {
+        const size_t n = (size_t)4 * (sl.nx + 2 * GC) * (sl.ny + 2 * GC) * sizeof(double);
+        CKS(cudaMemcpyAsync(U, sl.u, n, cudaMemcpyDeviceToHost, s->stream));
+    }
+    CKS(cudaFreeAsync(sl.u, s->stream));
+    CKS(cudaFreeAsync(sl.u1, s->stream));
+    CKS(cudaFreeAsync(sl.u2, s->stream));
+    CKS(cudaFreeAsync(sl.partials, s->stream));
+    CKS(cudaStreamSynchronize(s->stream));
+    memset(&s->h_desc[q], 0, sizeof(SlotDesc));
+    s->used -= sl.bytes;
+    sl = Slot();
+    s->dirty = true;
+    return EB2_OK;
+}
+
+int eb2_server_stats(eb2_server* s, unsigned long long* hbm_used, int* active,
+                     long long* graph_launches) {
+    if (!s) return fail(EB2_EARG, "null server");
+    int a = 0;
+    for (const Slot& sl : s->slots) a += sl.used && !sl.done;
+    if (hbm_used) *hbm_used = s->used;
+    if (active) *active = a;
+    if (graph_launches) *graph_launches = s->graph_launches;
+    return EB2_OK;
+}
+
+// Replay a request trace in real time: requests arrive at arrival_s[i]
+// seconds after the call starts, wait in FIFO order until a slot and the HBM
+// budget admit them, run in the batch, and are retired as they finish.
+int eb2_server_run_trace(eb2_server* s, const eb2_request* reqs, const double* arrival_s, int n,
+                         double* admit_s, double* finish_s, double** results,
+                         double* makespan_s) {
+    if (!s || (!reqs && n) || (!arrival_s && n)) return fail(EB2_EARG, "null argument");
+    CKS(cudaSetDevice(s->device));
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return arrival_s[a] < arrival_s[b]; });
+    std::map<long long, int> owner;  // request id -> trace index
+    std::vector<int> queue;
+    size_t next = 0, qhead = 0;
+    int completed = 0;
+    const double t0 = now_s();
+    while (completed < n) {
+        double t = now_s() - t0;
+        while (next < order.size() && arrival_s[order[next]] <= t) queue.push_back(order[next++]);
+        while (qhead < queue.size()) {
+            long long id;
+            int i = queue[qhead];
+            int rc = eb2_server_submit(s, &reqs[i], &id);
+            if (rc == EB2_EBUSY) break;
+            if (rc) return rc;
+            owner[id] = i;
+            if (admit_s) admit_s[i] = now_s() - t0;
+            qhead++;
+        }
+        int active = 0;
+        for (const Slot& sl : s->slots) active += sl.used && !sl.done;
+        if (!active) {
+            if (qhead < queue.size()) return fail(EB2_EBUSY, "a request never fits the budget");
+            if (next < order.size()) {
+                double wait = arrival_s[order[next]] - (now_s() - t0);
+                if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
+            }
+            continue;
+        }
+        int nf = 0;
+        if (int rc = eb2_server_step(s, 1, &nf)) return rc;
+        if (!nf) continue;
+        const double tf = now_s() - t0;
+        for (int q = 0; q < s->nslots; q++) {
+            Slot& sl = s->slots[q];
+            if (!sl.used || !sl.done) continue;
+            int i = owner[sl.id];
+            if (finish_s) finish_s[i] = tf;
+            if (int rc = eb2_server_fetch(s, sl.id, results ? results[i] : nullptr)) return rc;
+            completed++;
+        }
+    }
+    if (makespan_s) *makespan_s = now_s() - t0;
+    return EB2_OK;
+}
+
+}  // extern "C"

@@ -38,7 +38,7 @@ constexpr size_t smem_bytes() {
 }
 
 // rho > 0 and p > 0 without a division: 2*rho*E > (rho u)^2 + (rho v)^2.
-__device__ __forceinline__ bool admissible(const double* q) {
+EB2_HD bool admissible(const double* q) {
     return q[0] > 0.0 && 2.0 * q[3] * q[0] > q[1] * q[1] + q[2] * q[2];
 }
 
@@ -46,7 +46,7 @@ __device__ __forceinline__ bool admissible(const double* q) {
 // `stride` steps along the sweep, fields are FS apart.  pa/pb point at the
 // primitive 5-tuples of the two cells next to the interface (fields PS apart).
 template <int DIR, int RECON, bool CHAR, bool WZ, int FLUX>
-__device__ __forceinline__ unsigned interface_flux(const double* __restrict__ s, int stride,
+EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
                                                    const double* __restrict__ pa,
                                                    const double* __restrict__ pb, double delta,
                                                    const Gas& g, int positivity,
@@ -115,7 +115,7 @@ __device__ __forceinline__ unsigned interface_flux(const double* __restrict__ s,
     if (!x64::riemann<FLUX, DIR>(ql, qr, g, F)) {
         // the reference leaves a stale entry here; a NaN makes it visible
 #pragma unroll
-        for (int k = 0; k < 4; k++) F[k] = __longlong_as_double(0x7ff8000000000000ll);
+        for (int k = 0; k < 4; k++) F[k] = nan("");
         st |= ST_NONPHYSICAL;
     }
 #pragma unroll
@@ -123,8 +123,10 @@ __device__ __forceinline__ unsigned interface_flux(const double* __restrict__ s,
     return st;
 }
 
+// One tile (ti, tj) of one stage; tiles_x = tiles along y (for the partials
+// index).  Shared by the single-solve kernel and the batched kernel.
 template <int RECON, bool CHAR, bool WZ, int FLUX>
-__global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
+__device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, int tiles_x) {
     Ctrl* ctrl = a.ctrl;
     if (!ctrl->active) return;
     extern __shared__ double sm[];
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
     __shared__ double red[3][NT / 32];
 
     const int rows = a.grid.rows, cols = a.grid.cols;
-    const int i0 = GC + blockIdx.y * TX, j0 = GC + blockIdx.x * TY;
+    const int i0 = GC + ti * TX, j0 = GC + tj * TY;
     const double* __restrict__ uin = a.uin;
     const Gas g = a.gas;
 
@@ -262,12 +264,18 @@ __global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
                 if (red[1][q] > by) by = red[1][q];
                 bp += red[2][q];
             }
-            size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+            size_t b = (size_t)ti * tiles_x + tj;
             a.partials[3 * b + 0] = bx;
             a.partials[3 * b + 1] = by;
             a.partials[3 * b + 2] = bp;
         }
     }
+}
+
+// Single solve: one CTA per tile.
+template <int RECON, bool CHAR, bool WZ, int FLUX>
+__global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
+    stage_tile<RECON, CHAR, WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 template <int RECON, bool CHAR, bool WZ, int FLUX>

@@ -34,7 +34,7 @@ constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS) * sizeof(float) +
 // along the sweep); pa/pb: primitive records of cells i and i+1 (fields PS
 // apart); ga/gb: the two cells in global memory (near-vacuum path).
 template <int DIR, bool WZ, int FLUX>
-__device__ __forceinline__ unsigned interface_flux(const float* __restrict__ s, int stride,
+EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
                                                    const float* __restrict__ pa,
                                                    const float* __restrict__ pb,
                                                    const double* __restrict__ u, size_t ga,
@@ -78,18 +78,19 @@ __device__ __forceinline__ unsigned interface_flux(const float* __restrict__ s, 
     float dqm[4], dqp[4];
     f32::unproject<DIR>(e, wm, dqm);
     f32::unproject<DIR>(e, wp, dqp);
-    const float rb = pa[f32::P_RHO * PS], ub = pa[f32::P_U * PS], vb = pa[f32::P_V * PS],
-                pbs = pa[f32::P_P * PS];
-    f32::Prim L = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, dqm, gm1);
-    f32::Prim R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, dqp, gm1);
+    // minus side around cell i, plus side around cell i+1
+    const float ra = pa[f32::P_RHO * PS], ua = pa[f32::P_U * PS], va = pa[f32::P_V * PS],
+                pas = pa[f32::P_P * PS];
+    const float rb = pb[f32::P_RHO * PS], ub = pb[f32::P_U * PS], vb = pb[f32::P_V * PS],
+                pbs = pb[f32::P_P * PS], eb = s[3 * FS + 3 * stride];
+    f32::Prim L = f32::prim_from_delta<DIR>(ra, ua, va, pas, b3, dqm, gm1);
+    f32::Prim R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, eb, dqp, gm1);
     unsigned st = 0;
     if (!(L.r > 0.0f && L.p > 0.0f && R.r > 0.0f && R.p > 0.0f)) {
         if (positivity) {
             float z[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            float d[4] = {s[3 * stride] - b0, s[FS + 3 * stride] - b1,
-                          s[2 * FS + 3 * stride] - b2, s[3 * FS + 3 * stride] - b3};
-            L = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, z, gm1);
-            R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, b3, d, gm1);
+            L = f32::prim_from_delta<DIR>(ra, ua, va, pas, b3, z, gm1);
+            R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, eb, z, gm1);
         } else {
             st |= ST_NONPHYSICAL;
         }
@@ -107,8 +108,9 @@ __device__ __forceinline__ unsigned interface_flux(const float* __restrict__ s, 
     return st;
 }
 
+// One tile (ti, tj) of one stage; shared by the single-solve and batched kernels.
 template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
+__device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, int tiles_x) {
     Ctrl* ctrl = a.ctrl;
     if (!ctrl->active) return;
     extern __shared__ double smd[];
@@ -120,7 +122,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
 
     const int rows = a.grid.rows, cols = a.grid.cols;
     const size_t plane = (size_t)rows * cols;
-    const int i0 = GC + blockIdx.y * TX, j0 = GC + blockIdx.x * TY;
+    const int i0 = GC + ti * TX, j0 = GC + tj * TY;
     const double* __restrict__ uin = a.uin;
     const Gas g = a.gas;
     const float pthr = (float)(1.0e-3 * ctrl->pmean);
@@ -138,19 +140,7 @@ __global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
 #pragma unroll
         for (int k = 0; k < 4; k++) sU[k * FS + e] = (float)q[k];
         int pr = r - 2, pc = c - 2;
-        if (pr >= 0 && pr < PX && pc >= 0 && pc < PY) {
-            double rho = q[0];
-            double ir = 1.0 / rho;
-            double uu = q[1] * ir, vv = q[2] * ir;
-            double p = (q[3] - 0.5 * (q[1] * uu + q[2] * vv)) * g.gm1;
-            int pe = pr * PY + pc;
-            sP[f32::P_RHO * PS + pe] = (float)rho;
-            sP[f32::P_U * PS + pe] = (float)uu;
-            sP[f32::P_V * PS + pe] = (float)vv;
-            sP[f32::P_P * PS + pe] = (float)p;
-            sP[f32::P_H * PS + pe] = (float)(g.gr * p * ir);
-            sP[f32::P_SR * PS + pe] = (float)sqrt(rho);
-        }
+        if (pr >= 0 && pr < PX && pc >= 0 && pc < PY) f32::cell_prims(q, g, sP + pr * PY + pc, PS);
     }
     __syncthreads();
 
@@ -255,12 +245,18 @@ __global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
                 if (red[1][q] > by) by = red[1][q];
                 bp += red[2][q];
             }
-            size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+            size_t b = (size_t)ti * tiles_x + tj;
             a.partials[3 * b + 0] = bx;
             a.partials[3 * b + 1] = by;
             a.partials[3 * b + 2] = bp;
         }
     }
+}
+
+// Single solve: one CTA per tile.
+template <bool WZ, int FLUX>
+__global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
+    stage_tile<WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 template <bool WZ, int FLUX>

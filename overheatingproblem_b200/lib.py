@@ -15,7 +15,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_NAME = "libeuler_b200.so"
 
-EB2_OK, EB2_EARG, EB2_ENOMEM, EB2_ECUDA, EB2_ENONPHYS, EB2_EUNSUPPORTED = range(6)
+EB2_OK, EB2_EARG, EB2_ENOMEM, EB2_ECUDA, EB2_ENONPHYS, EB2_EUNSUPPORTED, EB2_EBUSY = range(7)
 ST_NONPHYSICAL, ST_NAN_STATE, ST_BAD_DT = 1, 2, 4
 FP64, MIXED = 0, 1
 BC_OUTFLOW, BC_REFLECTION, BC_PERIODICITY, BC_INFLOW, BC_FIXED_VALUE = range(5)
@@ -51,6 +51,13 @@ class Control(C.Structure):
     ]
 
 
+class Request(C.Structure):
+    """eb2_request of include/euler_b200.h."""
+    _fields_ = [("test_case", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("has_q", C.c_int),
+                ("q", C.c_double * 16), ("lx", C.c_double), ("ly", C.c_double),
+                ("tmax", C.c_double), ("cfl", C.c_double)]
+
+
 # name -> (restype, argtypes); every entry point declared in include/euler_b200.h
 SIGNATURES = {
     "eb2_ctx_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.c_int, C.c_int]),
@@ -61,9 +68,11 @@ SIGNATURES = {
     "eb2_set_precision": (C.c_int, [_vp, C.c_int]),
     "eb2_set_positivity_fallback": (C.c_int, [_vp, C.c_int]),
     "eb2_set_bc": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "eb2_get_bc": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "eb2_set_bc_states": (C.c_int, [_vp, _dp, _dp]),
     "eb2_set_double_mach": (C.c_int, [_vp, C.c_int]),
     "eb2_init_case": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp]),
+    "eb2_init_case_fields": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "eb2_upload": (C.c_int, [_vp, _dp]),
     "eb2_download": (C.c_int, [_vp, _dp]),
     "eb2_state_device_ptr": (C.c_int, [_vp, C.POINTER(_dp)]),
@@ -73,7 +82,7 @@ SIGNATURES = {
     "eb2_reconstruct": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _dp, _dp]),
     "eb2_riemann": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, _dp]),
     "eb2_flux_reconstruction": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _dp, _dp]),
-    "eb2_space_discrete": (C.c_int, [_vp, C.c_double, C.c_double, _dp, _dp, _dp]),
+    "eb2_space_discrete": (C.c_int, [_vp, C.c_double, C.c_double, _dp, _dp, _dp, _dp]),
     "eb2_delta_t": (C.c_int, [_vp, C.c_double, C.c_double, _dp]),
     "eb2_wave_speeds": (C.c_int, [_vp, _dp, _dp]),
     "eb2_rk_step": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -84,6 +93,18 @@ SIGNATURES = {
     "eb2_bench_steps": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                   C.c_ulonglong, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                   C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "eb2_server_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.c_int, C.c_ulonglong, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]),
+    "eb2_server_destroy": (C.c_int, [_vp]),
+    "eb2_server_submit": (C.c_int, [_vp, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "eb2_server_step": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
+    "eb2_server_poll": (C.c_int, [_vp, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_longlong),
+                                  C.POINTER(C.c_uint), C.c_int, C.POINTER(C.c_int)]),
+    "eb2_server_fetch": (C.c_int, [_vp, C.c_longlong, _dp]),
+    "eb2_server_stats": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_longlong)]),
+    "eb2_server_run_trace": (C.c_int, [_vp, C.POINTER(Request), _dp, C.c_int, _dp, _dp,
+                                       C.POINTER(_dp), _dp]),
     "eb2_status": (C.c_int, [_vp, C.POINTER(C.c_uint)]),
     "eb2_clear_status": (C.c_int, [_vp]),
     "eb2_synchronize": (C.c_int, [_vp]),

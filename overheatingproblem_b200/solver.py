@@ -135,9 +135,10 @@ class Solver:
         L.check(self._lib.eb2_flux_reconstruction(self._h, scheme, dx, dy, L.dptr(f), L.dptr(g)))
         return f, g
 
-    def space_discrete(self, dx, dy, f, g, out=None):
+    def space_discrete(self, dx, dy, f, g, out=None, source=None):
         out = self.zeros() if out is None else out
-        L.check(self._lib.eb2_space_discrete(self._h, dx, dy, L.dptr(f), L.dptr(g),
+        src = None if source is None else L.dptr(np.ascontiguousarray(source))
+        L.check(self._lib.eb2_space_discrete(self._h, dx, dy, L.dptr(f), L.dptr(g), src,
                                              L.dptr(out)))
         return out
 

@@ -1,0 +1,86 @@
+// eb2_pointcheck.cu -- CPU access to the per-interface routines of both
+// stage kernels, for tests that compare the mixed-precision face arithmetic
+// with the FP64 face arithmetic without a GPU.  Host code only: the routines
+// are the same host+device templates the kernels instantiate, fed from arrays
+// laid out with the kernels' shared-memory strides.
+#include "eb2_stage_fp64.cuh"
+#include "eb2_stage_mixed.cuh"
+
+using namespace eb2;
+
+namespace {
+
+template <int DIR, int RECON, bool CH, bool WZ, int FLUX>
+unsigned fp64_face(const double* cells, double delta, const Gas& g, int pos, double* F) {
+    static double sU[4 * fp64stage::FS], sP[5 * fp64stage::PS];
+    for (int n = 0; n < 6; n++)
+        for (int k = 0; k < 4; k++) sU[k * fp64stage::FS + n] = cells[4 * n + k];
+    double w[5];
+    for (int c = 0; c < 2; c++) {
+        const double* q = cells + 4 * (2 + c);
+        x64::primitive5(q[0], q[1], q[2], q[3], g, w);
+        for (int k = 0; k < 5; k++) sP[k * fp64stage::PS + c] = w[k];
+    }
+    return fp64stage::interface_flux<DIR, RECON, CH, WZ, FLUX>(sU, 1, sP, sP + 1, delta, g, pos,
+                                                               F, 1);
+}
+
+template <int DIR, bool WZ, int FLUX>
+unsigned mixed_face(const double* cells, double pthr, const Gas& g, int pos, double* F) {
+    static float sU[4 * mixstage::FS], sP[f32::NP * mixstage::PS];
+    for (int n = 0; n < 6; n++)
+        for (int k = 0; k < 4; k++) sU[k * mixstage::FS + n] = (float)cells[4 * n + k];
+    double u[8];
+    for (int c = 0; c < 2; c++) {
+        f32::cell_prims(cells + 4 * (2 + c), g, sP + c, mixstage::PS);
+        for (int k = 0; k < 4; k++) u[c + 2 * k] = cells[4 * (2 + c) + k];
+    }
+    return mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, sP, sP + 1, u, 0, 1, 2, (float)pthr, g,
+                                                   pos, F, 1);
+}
+
+template <int DIR, int RECON, bool CH, bool WZ>
+unsigned fp64_by_flux(int flux, const double* c, double d, const Gas& g, int pos, double* F) {
+    switch (flux) {
+        case FLUX_HLL: return fp64_face<DIR, RECON, CH, WZ, FLUX_HLL>(c, d, g, pos, F);
+        case FLUX_HLLC: return fp64_face<DIR, RECON, CH, WZ, FLUX_HLLC>(c, d, g, pos, F);
+        case FLUX_ROE: return fp64_face<DIR, RECON, CH, WZ, FLUX_ROE>(c, d, g, pos, F);
+        default: return fp64_face<DIR, RECON, CH, WZ, FLUX_LLF>(c, d, g, pos, F);
+    }
+}
+
+template <int DIR, bool WZ>
+unsigned mixed_by_flux(int flux, const double* c, double pthr, const Gas& g, int pos, double* F) {
+    switch (flux) {
+        case FLUX_HLL: return mixed_face<DIR, WZ, FLUX_HLL>(c, pthr, g, pos, F);
+        case FLUX_HLLC: return mixed_face<DIR, WZ, FLUX_HLLC>(c, pthr, g, pos, F);
+        case FLUX_ROE: return mixed_face<DIR, WZ, FLUX_ROE>(c, pthr, g, pos, F);
+        default: return mixed_face<DIR, WZ, FLUX_LLF>(c, pthr, g, pos, F);
+    }
+}
+
+Gas gas_of(double gamma) { return Gas{gamma, gamma - 1.0, gamma / (gamma - 1.0)}; }
+
+}  // namespace
+
+// cells: 6 conserved states (rho, rho u, rho v, rho E) of cells i-2..i+3 along
+// the sweep; F: the flux at face i+1/2.  Characteristic WENO5 only.
+extern "C" unsigned pc_face_fp64(int dir, int weno_z, int flux, double gamma, const double* cells,
+                                 double delta, int positivity, double* F) {
+    Gas g = gas_of(gamma);
+    if (dir == 1)
+        return weno_z ? fp64_by_flux<1, 5, true, true>(flux, cells, delta, g, positivity, F)
+                      : fp64_by_flux<1, 5, true, false>(flux, cells, delta, g, positivity, F);
+    return weno_z ? fp64_by_flux<2, 5, true, true>(flux, cells, delta, g, positivity, F)
+                  : fp64_by_flux<2, 5, true, false>(flux, cells, delta, g, positivity, F);
+}
+
+extern "C" unsigned pc_face_mixed(int dir, int weno_z, int flux, double gamma,
+                                  const double* cells, double pthr, int positivity, double* F) {
+    Gas g = gas_of(gamma);
+    if (dir == 1)
+        return weno_z ? mixed_by_flux<1, true>(flux, cells, pthr, g, positivity, F)
+                      : mixed_by_flux<1, false>(flux, cells, pthr, g, positivity, F);
+    return weno_z ? mixed_by_flux<2, true>(flux, cells, pthr, g, positivity, F)
+                  : mixed_by_flux<2, false>(flux, cells, pthr, g, positivity, F);
+}

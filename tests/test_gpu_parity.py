@@ -136,6 +136,10 @@ def test_granular_operators(gpu):
         assert same_bits(f[fx], z["f"][fx]) and same_bits(g[gy], z["g"][gy])
         Lt = s.space_discrete(dx, dy, z["f"], z["g"])
         assert same_bits(interior(Lt), interior(z["L"]))
+        # a caller-given source array is added last, as Space_Discrete_Item's s
+        src = np.random.default_rng(5).standard_normal(z["L"].shape)
+        Ls = s.space_discrete(dx, dy, z["f"], z["g"], source=src)
+        assert same_bits(interior(Ls), interior(z["L"] + src))
 
 
 def test_boundary_kinds(gpu):
