@@ -117,12 +117,15 @@ def serve_stream(eb2, local, n, rate, seed, baseline_n):
     lat = out["finish"] - arr
     batched = {"solves_per_s": n / out["makespan"], "makespan_s": out["makespan"],
                "p50_latency_s": float(np.percentile(lat, 50)),
-               "p99_latency_s": float(np.percentile(lat, 99)), "requests": n}
+               "p99_latency_s": float(np.percentile(lat, 99)), "requests": n,
+               "steps": int(out["steps"].sum()),
+               "non_physical": int((out["status"] != 0).sum())}
     # one-at-a-time plain FP64 launches: each request on its own context,
     # started when it has arrived and the previous one has finished
     m = min(baseline_n, n)
     t0 = time.perf_counter()
     fin = np.zeros(m)
+    bad = 0
     for i in range(m):
         wait = arr[i] - (time.perf_counter() - t0)
         if wait > 0:
@@ -134,44 +137,71 @@ def serve_stream(eb2, local, n, rate, seed, baseline_n):
             ly = r.ly if r.ly > 0 else ly
             s.run(ORDER, 2, lx / r.nx, ly / r.ny, r.tmax)
             s.download()
+            bad += s.status() != 0
         fin[i] = time.perf_counter() - t0
     blat = fin - arr[:m]
     base = {"solves_per_s": m / fin[-1], "makespan_s": float(fin[-1]),
             "p50_latency_s": float(np.percentile(blat, 50)),
-            "p99_latency_s": float(np.percentile(blat, 99)), "requests": m}
+            "p99_latency_s": float(np.percentile(blat, 99)), "requests": m,
+            "non_physical": int(bad)}
     return {"trace": f"{n} requests, Poisson arrivals at {rate}/s, seed {seed}",
             "batched_mixed": batched, "one_at_a_time_fp64": base,
             "speedup_solves_per_s": batched["solves_per_s"] / base["solves_per_s"]}
 
 
 def run_accuracy(args, local):
-    """FP64 vs mixed on the benchmark problem to t = T: density/velocity/pressure
-    L1 (mean over cells) and Linf differences, steps and device-loop time."""
+    """FP64 vs mixed on the benchmark problem up to t = T, with checkpoints:
+    density/velocity/pressure L1 (mean over cells) and Linf differences.  A
+    third run, FP64 from the same initial state with one density value moved
+    by one ulp, measures how far the flow itself amplifies a perturbation of
+    rounding size (the floor no arithmetic can go below)."""
     import numpy as np
     import torch
 
     import overheatingproblem_b200 as eb2
 
-    nx, scheme = args.nx, SCHEMES[args.scheme]
+    nx, scheme, T = args.nx, SCHEMES[args.scheme], args.accuracy
+    marks = [t for t in (0.05, 0.1, 0.2) if t < T] + [T]
+    runs = {"fp64": eb2.lib.FP64, "mixed": eb2.lib.MIXED, "fp64_1ulp": eb2.lib.FP64}
     out, prim = {}, {}
-    for prec in ("fp64", "mixed"):
+    for name, prec in runs.items():
         s = eb2.Solver(nx, nx, device=local, recon=5, characteristic=True, weno_z=False,
-                       cfl=0.5, precision=eb2.lib.FP64 if prec == "fp64" else eb2.lib.MIXED)
+                       cfl=0.5, precision=prec)
         lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+        if name == "fp64_1ulp":
+            U = s.download()
+            c = 4 + nx // 3
+            U[0, c, c] = np.nextafter(U[0, c, c], np.inf)
+            s.upload(U)
         torch.cuda.synchronize(local)
-        t0 = time.perf_counter()
-        n, tf = s.run(ORDER, scheme, lx / nx, ly / nx, args.accuracy)
-        el = time.perf_counter() - t0
-        prim[prec] = s.con_to_pri()[:, 4:-4, 4:-4].copy()
-        out[prec] = {"steps": n, "t_final": tf, "seconds": el, "status_flags": s.status(),
-                     "cell_updates_per_s": nx * nx * n / el}
+        el, steps, t = 0.0, 0, 0.0
+        prim[name] = []
+        for tm in marks:
+            t0 = time.perf_counter()
+            n, t = s.run(ORDER, scheme, lx / nx, ly / nx, tm, t0=t)
+            el += time.perf_counter() - t0
+            steps += n
+            prim[name].append(s.con_to_pri()[:, 4:-4, 4:-4].copy())
+        out[name] = {"steps": steps, "t_final": t, "seconds": el, "status_flags": s.status(),
+                     "cell_updates_per_s": nx * nx * steps / el}
         s.close()
-    d = np.abs(prim["fp64"] - prim["mixed"])
     names = ["rho", "u", "v", "p"]
-    line = {"accuracy": workload(nx, "mixed", args.scheme) + f" vs FP64, t = {args.accuracy}",
-            "l1": {k: float(d[i].mean()) for i, k in enumerate(names)},
-            "linf": {k: float(d[i].max()) for i, k in enumerate(names)},
-            "rel_l1_rho": float(d[0].sum() / np.abs(prim["fp64"][0]).sum()),
+
+    def diff(other):
+        rows = []
+        for k, tm in enumerate(marks):
+            d = np.abs(prim["fp64"][k] - prim[other][k])
+            rows.append({"t": tm, "l1": {q: float(d[i].mean()) for i, q in enumerate(names)},
+                         "linf": {q: float(d[i].max()) for i, q in enumerate(names)}})
+        return rows
+
+    mixed, ulp = diff("mixed"), diff("fp64_1ulp")
+    line = {"accuracy": workload(nx, "mixed", args.scheme) + f" vs FP64, t = {T}",
+            "l1": mixed[-1]["l1"], "linf": mixed[-1]["linf"],
+            "rel_l1_rho": float(np.abs(prim["fp64"][-1][0] - prim["mixed"][-1][0]).sum() /
+                                np.abs(prim["fp64"][-1][0]).sum()),
+            "checkpoints": {"mixed_vs_fp64": mixed, "fp64_1ulp_vs_fp64": ulp},
+            "note": "checkpoint times clip the CFL step in all three runs alike",
             "runs": out}
     print(json.dumps(line), flush=True)
 

@@ -256,11 +256,11 @@ int eb2_server_stats(eb2_server *srv, unsigned long long *hbm_used, int *active,
 /* The request loop: replay n requests arriving arrival_s[i] seconds after the
  * call in real time (FIFO admission by slot and budget, batch steps, retire as
  * finished).  Per request: admission and finish times in seconds since the
- * start (either array may be NULL) and, when results != NULL and results[i]
- * != NULL, the final state. */
+ * start, step counts and status bits (EB2_ST_*; any of these arrays may be
+ * NULL) and, when results != NULL and results[i] != NULL, the final state. */
 int eb2_server_run_trace(eb2_server *srv, const eb2_request *reqs, const double *arrival_s,
-                         int n, double *admit_s, double *finish_s, double **results,
-                         double *makespan_s);
+                         int n, double *admit_s, double *finish_s, long long *steps,
+                         unsigned *status, double **results, double *makespan_s);
 
 /* --- diagnostics ------------------------------------------------------------- */
 

@@ -40,7 +40,7 @@ CUDA_SOURCES = [
     ("eb2_stage_mixed.cu", False),
     ("eb2_batch_mixed.cu", False),
 ]
-C_SOURCES = ["eb2_control.c"]
+C_SOURCES = ["eb2_control.c", "rpf_runtime.c"]
 HEADERS = ["eb2_common.cuh", "eb2_kernels.h", "eb2_point_fp64.cuh", "eb2_stage_fp64.cuh",
            "eb2_point_mixed.cuh", "eb2_stage_mixed.cuh", "eb2_loop.cuh", "eb2_batch.cuh"]
 
@@ -58,7 +58,9 @@ def _newest_header() -> float:
         p = os.path.join(CSRC, h)
         if os.path.exists(p):
             t = max(t, os.path.getmtime(p))
-    return max(t, os.path.getmtime(os.path.join(INCLUDE, "euler_b200.h")))
+    for h in ("euler_b200.h", os.path.join("rp_fvm", "rpf_runtime.h")):
+        t = max(t, os.path.getmtime(os.path.join(INCLUDE, h)))
+    return t
 
 
 def _stale(src: str, obj: str, hdr_time: float) -> bool:
@@ -80,7 +82,7 @@ def _compile_cuda(src: str, exact: bool, log: list) -> str:
 
 def _compile_c(src: str, log: list) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    cmd = ["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", "-c", src, "-o", obj]
+    cmd = ["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", "-I", INCLUDE, "-c", src, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     log.append((src, res.stdout + res.stderr))
     if res.returncode:

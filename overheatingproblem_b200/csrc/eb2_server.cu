@@ -490,8 +490,8 @@ int eb2_server_stats(eb2_server* s, unsigned long long* hbm_used, int* active,
 // seconds after the call starts, wait in FIFO order until a slot and the HBM
 // budget admit them, run in the batch, and are retired as they finish.
 int eb2_server_run_trace(eb2_server* s, const eb2_request* reqs, const double* arrival_s, int n,
-                         double* admit_s, double* finish_s, double** results,
-                         double* makespan_s) {
+                         double* admit_s, double* finish_s, long long* steps, unsigned* status,
+                         double** results, double* makespan_s) {
     if (!s || (!reqs && n) || (!arrival_s && n)) return fail(EB2_EARG, "null argument");
     CKS(cudaSetDevice(s->device));
     std::vector<int> order(n);
@@ -535,6 +535,8 @@ int eb2_server_run_trace(eb2_server* s, const eb2_request* reqs, const double* a
             if (!sl.used || !sl.done) continue;
             int i = owner[sl.id];
             if (finish_s) finish_s[i] = tf;
+            if (steps) steps[i] = sl.steps;
+            if (status) status[i] = sl.status;
             if (int rc = eb2_server_fetch(s, sl.id, results ? results[i] : nullptr)) return rc;
             completed++;
         }

@@ -104,6 +104,7 @@ SIGNATURES = {
     "eb2_server_stats": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_int),
                                    C.POINTER(C.c_longlong)]),
     "eb2_server_run_trace": (C.c_int, [_vp, C.POINTER(Request), _dp, C.c_int, _dp, _dp,
+                                       C.POINTER(C.c_longlong), C.POINTER(C.c_uint),
                                        C.POINTER(_dp), _dp]),
     "eb2_status": (C.c_int, [_vp, C.POINTER(C.c_uint)]),
     "eb2_clear_status": (C.c_int, [_vp]),

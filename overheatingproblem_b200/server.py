@@ -115,6 +115,8 @@ class Server:
         t_arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
         admit = np.zeros(n)
         finish = np.zeros(n)
+        steps = (C.c_longlong * max(n, 1))()
+        status = (C.c_uint * max(n, 1))()
         span = C.c_double()
         results = None
         res_ptrs = None
@@ -122,5 +124,8 @@ class Server:
             results = [np.zeros((4, r.nx + 8, r.ny + 8)) for r in reqs]
             res_ptrs = (_dp * n)(*[L.dptr(a) for a in results])
         L.check(self._lib.eb2_server_run_trace(self._h, arr, L.dptr(t_arr), n, L.dptr(admit),
-                                               L.dptr(finish), res_ptrs, C.byref(span)))
-        return {"admit": admit, "finish": finish, "makespan": span.value, "results": results}
+                                               L.dptr(finish), steps, status, res_ptrs,
+                                               C.byref(span)))
+        return {"admit": admit, "finish": finish, "makespan": span.value, "results": results,
+                "steps": np.array(steps[:n], dtype=np.int64),
+                "status": np.array(status[:n], dtype=np.uint32)}

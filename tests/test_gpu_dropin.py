@@ -1,0 +1,91 @@
+"""The drop-in boundary end to end.
+
+The reference's own caller, src/RP_FVM.c, is built twice without a change:
+against the reference's headers (oracle/_ref/rp_fvm_cpu, its OpenMP CPU path)
+and against the drop-in header set include/rp_fvm/ linked to libeuler_b200.so
+(oracle/_ref/rp_fvm_b200).  Both are driven by the same control files; the
+result files they write (Tecplot .plt / profile .dat at %.8f) must be the same
+bytes, and the accuracy test's error lines the same text.  Built by
+`make -C oracle dropin` where the reference tree is present.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+BIN = os.path.join(ROOT, "oracle", "_ref")
+CPU = os.path.join(BIN, "rp_fvm_cpu")
+GPU = os.path.join(BIN, "rp_fvm_b200")
+
+BASE = {"Time_ADM": 3, "scheme": 2, "M_gamma": 1.4, "Source": "false", "Gravity": 1.0,
+        "CFL": 0.5, "Tmax": 0.3, "Control_Compution": 0, "Control_output": 2,
+        "Recon_Accur": 5, "Characteriz": "false"}
+
+CASES = {
+    "riemann3_hllc_rk3": {"TestCase": "2D_Riemann_Case3", "L_nx": 48, "L_ny": 40},
+    "riemann4_hll_rk2": {"TestCase": "2D_Riemann_Case4", "L_nx": 40, "L_ny": 36,
+                         "Time_ADM": 2, "scheme": 1},
+    "riemann1_roe_rk1": {"TestCase": "2D_Riemann_Case1", "L_nx": 33, "L_ny": 29,
+                         "Time_ADM": 1, "scheme": 3},
+    "riemann2_llf_rk3": {"TestCase": "2D_Riemann_Case2", "L_nx": 40, "L_ny": 40, "scheme": 4},
+    "sod_hllc_rk3": {"TestCase": "1D_Sod_Shocktube", "L_nx": 100, "L_ny": 1},
+}
+
+
+def need_binaries():
+    if not (os.path.exists(CPU) and os.path.exists(GPU)):
+        pytest.skip("drop-in binaries not built (make -C oracle dropin)")
+
+
+def run(binary, workdir, params, env_extra=None):
+    os.makedirs(workdir, exist_ok=True)
+    ctl = os.path.join(workdir, "control.txt")
+    with open(ctl, "w") as fh:
+        for k, v in {**BASE, **params, "output_dir": "out"}.items():
+            fh.write(f"{k}: {v}\n")
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(16, os.cpu_count() or 1)))
+    env.update(env_extra or {})
+    res = subprocess.run([binary, "control.txt"], cwd=workdir, env=env, capture_output=True,
+                         text=True, errors="replace", timeout=600)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+    out = os.path.join(workdir, "out")
+    files = sorted(os.listdir(out)) if os.path.isdir(out) else []
+    return res.stdout, {f: open(os.path.join(out, f), "rb").read() for f in files}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reference_caller_writes_the_same_files(tmp_path, name):
+    need_binaries()
+    _, ref = run(CPU, str(tmp_path / "cpu"), CASES[name])
+    _, gpu = run(GPU, str(tmp_path / "gpu"), CASES[name])
+    assert ref and sorted(ref) == sorted(gpu)
+    for f in ref:
+        assert ref[f] == gpu[f], f
+
+
+def test_strict_coherence_mode_gives_the_same_files(tmp_path):
+    need_binaries()
+    params = CASES["riemann3_hllc_rk3"]
+    _, ref = run(GPU, str(tmp_path / "resident"), params)
+    _, strict = run(GPU, str(tmp_path / "strict"), params, {"RPF_COHERENCE": "strict"})
+    assert ref == strict
+
+
+def test_accuracy_test_prints_the_same_errors(tmp_path):
+    """Precision_test (src/RP_FVM.c:974-1072): Init_Precision, the fixed
+    step, RK3 on seven grids, then the error norms and the order table."""
+    need_binaries()
+    params = {"TestCase": "Precision_Test", "L_nx": 10, "L_ny": 1}
+    pat = re.compile(r"(L1 Error|L2 Error|L∞ Error) = \S+|^\d+ +\S+ +\S+.*$", re.M)
+    ref, _ = run(CPU, str(tmp_path / "cpu"), params)
+    gpu, _ = run(GPU, str(tmp_path / "gpu"), params)
+    lines_a = [m.group(0) for m in pat.finditer(ref)]
+    lines_b = [m.group(0) for m in pat.finditer(gpu)]
+    assert len(lines_a) == 28 and lines_a == lines_b   # 7 grids x 3 norms + 7 table rows
