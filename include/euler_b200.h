@@ -262,6 +262,40 @@ int eb2_server_run_trace(eb2_server *srv, const eb2_request *reqs, const double 
                          int n, double *admit_s, double *finish_s, long long *steps,
                          unsigned *status, double **results, double *makespan_s);
 
+/* --- step without allocation ------------------------------------------------ */
+
+/* No counterpart in the reference.  Some callers cannot call cudaMalloc at
+ * all: a host application whose own pool owns all device memory, a real-time
+ * loop that forbids allocation after start-up, a plug-in that is only handed
+ * device pointers.  eb2_rk_step_noalloc runs one RK1/RK2/RK3 step of the FP64
+ * form (the same kernels as eb2_rk_step, the same bits) on a state U that the
+ * caller holds in device memory, [4][nx+8][ny+8] in the layout above, updated
+ * in place, and allocates nothing: its scratch (two stage states and a control
+ * block) lives in one static __device__ array of the library, about 16 MiB,
+ * that every GPU which loads the library keeps until the process exits.
+ *
+ * Limits: (nx+8)*(ny+8) <= EB2_NOALLOC_MAX_CELLS, else EB2_EARG.  All calls
+ * share the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must not be issued.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  The call enqueues
+ * on `cuda_stream` (NULL: the legacy default stream) and returns after the
+ * step, with EB2_ENONPHYS if a non-physical state was met.  Nothing in the
+ * array has to start at zero: each call clears the control block itself, and
+ * every stage-buffer value a call reads was written earlier in that call.
+ * Boundary kinds use the reference's default inflow and fixed states. */
+#define EB2_NOALLOC_MAX_CELLS 262144
+typedef struct {
+    double gamma;
+    int recon, characteristic, weno_z;               /* as eb2_set_reconstruction */
+    int bc_left, bc_right, bc_bottom, bc_top;        /* EB2_BC_*                  */
+    int source;
+    double gravity;
+} eb2_noalloc_config;
+int eb2_rk_step_noalloc(double *U_device, int nx, int ny, const eb2_noalloc_config *cfg,
+                        int order, int scheme, double dt, double dx, double dy, double time,
+                        void *cuda_stream);
+
 /* --- diagnostics ------------------------------------------------------------- */
 
 int eb2_status(eb2_ctx *ctx, unsigned *flags);

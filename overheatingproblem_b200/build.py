@@ -35,6 +35,7 @@ CUDA_SOURCES = [
     ("eb2_stage.cu", True),
     ("eb2_aux.cu", True),
     ("eb2_api.cu", True),
+    ("eb2_noalloc.cu", True),
     ("eb2_batch_fp64.cu", True),
     ("eb2_server.cu", True),
     ("eb2_stage_mixed.cu", False),

@@ -58,6 +58,18 @@ class Request(C.Structure):
                 ("tmax", C.c_double), ("cfl", C.c_double)]
 
 
+class NoallocConfig(C.Structure):
+    """eb2_noalloc_config of include/euler_b200.h."""
+    _fields_ = [
+        ("gamma", C.c_double), ("recon", C.c_int), ("characteristic", C.c_int),
+        ("weno_z", C.c_int), ("bc_left", C.c_int), ("bc_right", C.c_int),
+        ("bc_bottom", C.c_int), ("bc_top", C.c_int), ("source", C.c_int),
+        ("gravity", C.c_double),
+    ]
+
+
+NOALLOC_MAX_CELLS = 262144
+
 # name -> (restype, argtypes); every entry point declared in include/euler_b200.h
 SIGNATURES = {
     "eb2_ctx_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.c_int, C.c_int]),
@@ -106,6 +118,9 @@ SIGNATURES = {
     "eb2_server_run_trace": (C.c_int, [_vp, C.POINTER(Request), _dp, C.c_int, _dp, _dp,
                                        C.POINTER(C.c_longlong), C.POINTER(C.c_uint),
                                        C.POINTER(_dp), _dp]),
+    "eb2_rk_step_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(NoallocConfig), C.c_int,
+                                      C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      _vp]),
     "eb2_status": (C.c_int, [_vp, C.POINTER(C.c_uint)]),
     "eb2_clear_status": (C.c_int, [_vp]),
     "eb2_synchronize": (C.c_int, [_vp]),
