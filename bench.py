@@ -220,6 +220,21 @@ def config(args):
             "parallelism": "replicas"}
 
 
+def measured_traffic(nx, precision, scheme):
+    """DRAM bytes (read + write) per fused-stage launch of this workload, from
+    the committed ncu launch-list summary profiles/launches_<precision>_<nx>.md
+    (taken with the same bench command), or None when there is none."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        f"launches_{precision}_{nx}.md")
+    if scheme != "hllc" or not os.path.exists(path):
+        return None
+    for line in open(path):
+        if "k_stage" in line and line.startswith("|"):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            return (float(cells[4].split()[0]) + float(cells[5].split()[0])) * 1e6
+    return None
+
+
 def hbm_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -413,7 +428,9 @@ def run_ours(args, world, rank, local):
     alg_bytes = nx * nx * BYTES_PER_CELL_STEP * args.steps
     achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
+                "frac": achieved / peak,
+                "traffic": measured_traffic(nx, args.precision, args.scheme),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch",
                 "kernel": f"eb2 fused x+y sweep + RK stage ({args.precision})",
                 "per_launch_ms": stage_ms / nstage, "peak_kind": peak_kind,
                 "alg_bytes_per_launch": nx * nx * BYTES_PER_CELL_STEP / ORDER,
