@@ -232,6 +232,12 @@ class Reference:
         self.configure(p)
         return self.lib.ref_dt(U.shape[1], U.shape[2], _ptr(U), dx, dy)
 
+    def riemann(self, p, scheme, direction, ql, qr, flux):
+        self.configure(p)
+        self.lib.ref_riemann(scheme, direction, ql.shape[1], ql.shape[2], _ptr(ql), _ptr(qr),
+                             _ptr(flux))
+        return flux
+
     def run(self, p, order, scheme, U, dx, dy, tmax, n_out=1):
         self.configure(p)
         tf = C.c_double()

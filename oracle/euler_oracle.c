@@ -549,10 +549,173 @@ static void flux_llf(int n, const double ql[4], const double qr[4], double gamma
     for (int k = 0; k < 4; k++) F[k] = 0.5 * (FL[k] + FR[k]) - 0.5 * sp * (UR[k] - UL[k]);
 }
 
+/* physical flux along n with total enthalpy H (the solvers' FL/FR) */
+static void phys(int n, const struct side *s, double H, double F[4]) {
+    if (n == 1) {
+        F[0] = s->r * s->u; F[1] = s->r * s->uu + s->p;
+        F[2] = s->r * s->v * s->u; F[3] = s->r * H * s->u;
+    } else {
+        F[0] = s->r * s->v; F[1] = s->r * s->u * s->v;
+        F[2] = s->r * s->vv + s->p; F[3] = s->r * H * s->v;
+    }
+}
+
+/* HLLHC_Flux, include/scheme.h:1860-2136: HLL with the energy term
+   (sl sr / (sr - sl)) (e_R - e_L) rho_HLL, e = p / (rho (gamma - 1));
+   the Roe sound-speed fallback on a NaN Einfeldt speed is live in the y
+   sweep only (:2085-2089) */
+static void flux_hllhc(int n, const double ql[4], const double qr[4], double gamma,
+                       double F[4]) {
+    const double gm1 = gamma - 1.0, gr = gamma / gm1, igm1 = 1.0 / gm1;
+    struct side Ls, Rs;
+    unpack(ql, gm1, &Ls);
+    unpack(qr, gm1, &Rs);
+    double aL = sqrt(gamma * Ls.p * Ls.ir), aR = sqrt(gamma * Rs.p * Rs.ir);
+    double HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+    double HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    double FL[4], FR[4];
+    phys(n, &Ls, HL, FL);
+    phys(n, &Rs, HR, FR);
+    double sqL = sqrt(Ls.r), sqR = sqrt(Rs.r), isum = 1.0 / (sqL + sqR);
+    double ubar = (sqL * Ls.u + sqR * Rs.u) * isum;
+    double vbar = (sqL * Ls.v + sqR * Rs.v) * isum;
+    double Hbar = (sqL * HL + sqR * HR) * isum;
+    double eta = 0.5 * sqL * sqR * isum * isum;
+    double dn = n == 1 ? Rs.u - Ls.u : Rs.v - Ls.v;
+    double d = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dn * dn);
+    if (n == 2 && isnan(d)) d = sqrt(gm1 * (Hbar - 0.5 * (ubar * ubar + vbar * vbar)));
+    double nb = n == 1 ? ubar : vbar;
+    double sl = nb - d, sr = nb + d;
+    double rho_hll = (sr * Rs.r - sl * Ls.r + FL[0] - FR[0]) / (sr - sl);
+    double eL = Ls.ir * Ls.p * igm1, eR = Rs.ir * Rs.p * igm1;
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    } else {
+        double idiff = 1.0 / (sr - sl), slsr = sl * sr;
+        const double UL[4] = {Ls.r, Ls.ru, Ls.rv, Ls.re}, UR[4] = {Rs.r, Rs.ru, Rs.rv, Rs.re};
+        for (int k = 0; k < 4; k++)
+            F[k] = (sr * FL[k] - sl * FR[k] + slsr * (UR[k] - UL[k])) * idiff;
+        F[3] = F[3] + (slsr * idiff) * (eR - eL) * rho_hll;
+    }
+}
+
+/* HLLCHC_Flux, include/scheme.h:2153-2471: HLLC (enthalpy sound speed in both
+   sweeps) with (sl sr / (sr - sl)) (e_R - e_L) times the star density factor
+   added to the energy flux of the star states */
+static void flux_hllchc(int n, const double ql[4], const double qr[4], double gamma,
+                        double F[4]) {
+    const double gm1 = gamma - 1.0, gr = gamma / gm1, igm1 = 1.0 / gm1;
+    struct side Ls, Rs;
+    unpack(ql, gm1, &Ls);
+    unpack(qr, gm1, &Rs);
+    double HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+    double HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    double aL = sqrt((gamma - 1.0) * (HL - 0.5 * (Ls.uu + Ls.vv)));
+    double aR = sqrt((gamma - 1.0) * (HR - 0.5 * (Rs.uu + Rs.vv)));
+    double FL[4], FR[4];
+    phys(n, &Ls, HL, FL);
+    phys(n, &Rs, HR, FR);
+    double sqL = sqrt(Ls.r), sqR = sqrt(Rs.r), ssum = sqL + sqR, isum = 1.0 / ssum;
+    double ubar = (sqL * Ls.u + sqR * Rs.u) * isum;
+    double vbar = (sqL * Ls.v + sqR * Rs.v) * isum;
+    double eta = 0.5 * sqL * sqR / (ssum * ssum);
+    double uL = n == 1 ? Ls.u : Ls.v, uR = n == 1 ? Rs.u : Rs.v;   /* normal */
+    double tL = n == 1 ? Ls.v : Ls.u, tR = n == 1 ? Rs.v : Rs.u;   /* tangential */
+    double d = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * (uR - uL) * (uR - uL));
+    double nb = n == 1 ? ubar : vbar;
+    double sl = nb - d, sr = nb + d;
+    double den = Ls.r * (sl - uL) - Rs.r * (sr - uR);
+    double ss = (Rs.p - Ls.p + Ls.r * uL * (sl - uL) - Rs.r * uR * (sr - uR)) / den;
+    double mL = Ls.r * (sl - uL) / (sl - ss), mR = Rs.r * (sr - uR) / (sr - ss);
+    double feL = Ls.re * Ls.ir + (ss - uL) * (ss + Ls.p / (Ls.r * (sl - uL)));
+    double feR = Rs.re * Rs.ir + (ss - uR) * (ss + Rs.p / (Rs.r * (sr - uR)));
+    double eL = Ls.ir * Ls.p * igm1, eR = Rs.ir * Rs.p * igm1;
+    double idiff = 1.0 / (sr - sl), slsr = sl * sr;
+    double corr = slsr * idiff * (eR - eL);
+    int kn = n == 1 ? 1 : 2, kt = n == 1 ? 2 : 1;
+    const double UL[4] = {Ls.r, Ls.ru, Ls.rv, Ls.re}, UR[4] = {Rs.r, Rs.ru, Rs.rv, Rs.re};
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sl < 0.0 && ss >= 0.0) {
+        F[0] = FL[0] + sl * (mL - Ls.r);
+        F[kn] = FL[kn] + sl * (mL * ss - UL[kn]);
+        F[kt] = FL[kt] + sl * (mL * tL - UL[kt]);
+        F[3] = FL[3] + sl * (mL * feL - Ls.re) + corr * mL;
+    } else if (ss < 0.0 && sr > 0.0) {
+        F[0] = FR[0] + sr * (mR - Rs.r);
+        F[kn] = FR[kn] + sr * (mR * ss - UR[kn]);
+        F[kt] = FR[kt] + sr * (mR * tR - UR[kt]);
+        F[3] = FR[3] + sr * (mR * feR - Rs.re) + corr * mR;
+    } else {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    }
+}
+
+/* RoeHC_Flux, include/scheme.h:2793-3109: Roe with 1/(2c^2 + 1e-12) and
+   1/(c^2 + 1e-12), minus 1/2 |u_n + c| (e_R - e_L) rho_bar on the energy flux;
+   returns 1 (interface left untouched) on a NaN Roe density (:2944-2947) */
+static int flux_roehc(int n, const double ql[4], const double qr[4], double gamma,
+                      double F[4]) {
+    const double gm1 = gamma - 1.0, gr = gamma / gm1, igm1 = 1.0 / gm1, eps = 1e-12;
+    struct side Ls, Rs;
+    unpack(ql, gm1, &Ls);
+    unpack(qr, gm1, &Rs);
+    double eL = Ls.ir * Ls.p * igm1, eR = Rs.ir * Rs.p * igm1;
+    double HL = 0.5 * (Ls.uu + Ls.vv) + gr * (Ls.p * Ls.ir);
+    double HR = 0.5 * (Rs.uu + Rs.vv) + gr * (Rs.p * Rs.ir);
+    double FL[4], FR[4];
+    phys(n, &Ls, HL, FL);
+    phys(n, &Rs, HR, FR);
+    double sqL = sqrt(Ls.r), sqR = sqrt(Rs.r), isum = 1.0 / (sqL + sqR);
+    double rbar = sqL * sqR;
+    double ubar = (sqL * Ls.u + sqR * Rs.u) * isum;
+    double vbar = (sqL * Ls.v + sqR * Rs.v) * isum;
+    double Hbar = (sqL * HL + sqR * HR) * isum;
+    double q2 = ubar * ubar + vbar * vbar;
+    double cbar = sqrt(gm1 * (Hbar - 0.5 * q2));
+    double nb = n == 1 ? ubar : vbar;
+    double lam[4] = {fabs(nb - cbar), fabs(nb), fabs(nb), fabs(nb + cbar)};
+    double drho = Rs.r - Ls.r, du = Rs.u - Ls.u, dv = Rs.v - Ls.v, dp = Rs.p - Ls.p;
+    double c2 = cbar * cbar;
+    double i2c2 = 1.0 / (2.0 * c2 + eps), ic2 = 1.0 / (c2 + eps);
+    double dn = n == 1 ? du : dv, dt_ = n == 1 ? dv : du;
+    double al[4] = {(dp - rbar * cbar * dn) * i2c2, drho - dp * ic2, rbar * dt_,
+                    (dp + rbar * cbar * dn) * i2c2};
+    double K[4][4];
+    if (n == 1) {
+        double k0[4] = {1.0, ubar - cbar, vbar, Hbar - ubar * cbar};
+        double k1[4] = {1.0, ubar, vbar, 0.5 * q2};
+        double k2[4] = {0.0, 0.0, 1.0, vbar};
+        double k3[4] = {1.0, ubar + cbar, vbar, Hbar + ubar * cbar};
+        memcpy(K[0], k0, sizeof k0); memcpy(K[1], k1, sizeof k1);
+        memcpy(K[2], k2, sizeof k2); memcpy(K[3], k3, sizeof k3);
+    } else {
+        double k0[4] = {1.0, ubar, vbar - cbar, Hbar - vbar * cbar};
+        double k1[4] = {1.0, ubar, vbar, 0.5 * q2};
+        double k2[4] = {0.0, 1.0, 0.0, ubar};
+        double k3[4] = {1.0, ubar, vbar + cbar, Hbar + vbar * cbar};
+        memcpy(K[0], k0, sizeof k0); memcpy(K[1], k1, sizeof k1);
+        memcpy(K[2], k2, sizeof k2); memcpy(K[3], k3, sizeof k3);
+    }
+    for (int c = 0; c < 4; c++) F[c] = 0.5 * (FL[c] + FR[c]);
+    for (int w = 0; w < 4; w++) {
+        double term = 0.5 * lam[w] * al[w];
+        for (int c = 0; c < 4; c++) F[c] -= term * K[w][c];
+    }
+    if (isnan(rbar)) return 1;
+    F[3] = F[3] - 0.5 * lam[3] * (eR - eL) * rbar;
+    return 0;
+}
+
 static int point_flux(int scheme, int n, const double ql[4], const double qr[4],
                       double gamma, double F[4]) {
     switch (scheme) {
         case 1: return flux_hll(n, ql, qr, gamma, F);
+        case 11: flux_hllhc(n, ql, qr, gamma, F); return 0;
+        case 22: flux_hllchc(n, ql, qr, gamma, F); return 0;
+        case 33: return flux_roehc(n, ql, qr, gamma, F);
         case 2: flux_hllc(n, ql, qr, gamma, F); return 0;
         case 3: flux_roe(n, ql, qr, gamma, F); return 0;
         default: flux_llf(n, ql, qr, gamma, F); return 0;

@@ -90,6 +90,9 @@ void ref_riemann(int scheme, int dir, int rows, int cols, double *ql, double *qr
         case 1: HLL_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
         case 2: HLLC_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
         case 3: Roe_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
+        case 11: HLLHC_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
+        case 22: HLLCHC_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
+        case 33: RoeHC_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
         default: LLF_Flux(dir, var, rows, cols, GhostCell, a, b, f); break;
     }
 }

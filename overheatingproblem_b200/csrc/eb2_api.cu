@@ -42,8 +42,9 @@ int map_scheme(int scheme, int* flux) {
         case 1: *flux = FLUX_HLL; return EB2_OK;
         case 2: *flux = FLUX_HLLC; return EB2_OK;
         case 3: *flux = FLUX_ROE; return EB2_OK;
-        case 11: case 22: case 33:
-            return fail(EB2_EUNSUPPORTED, "heat-conduction scheme %d is not implemented", scheme);
+        case 11: *flux = FLUX_HLLHC; return EB2_OK;
+        case 22: *flux = FLUX_HLLCHC; return EB2_OK;
+        case 33: *flux = FLUX_ROEHC; return EB2_OK;
         default: *flux = FLUX_LLF; return EB2_OK;  // CFD_convection.h:111-116
     }
 }
@@ -119,6 +120,14 @@ void set_spacing(eb2_ctx* c, double dx, double dy) {
     c->grid.dy = dy;
     c->grid.inv_dx = 1.0 / dx;  // Space_Discrete_Item's inv_dx (scheme.h:3762)
     c->grid.inv_dy = 1.0 / dy;
+}
+
+// The mixed form implements the four classical fluxes only.
+int check_precision_flux(const eb2_ctx* c, int flux) {
+    if (c->precision == EB2_MIXED && flux >= FLUX_HLLHC)
+        return fail(EB2_EUNSUPPORTED,
+                    "the mixed form has no heat-conduction fluxes (AR_scheme 11/22/33)");
+    return EB2_OK;
 }
 
 int ensure_tmp(eb2_ctx* c, int n) {
@@ -649,6 +658,7 @@ int eb2_rk_step(eb2_ctx* c, int order, int scheme, double dt, double dx, double 
     if (order < 1 || order > 3) return fail(EB2_EARG, "Error: Invalid time advancement method");
     int flux;
     if (int r = map_scheme(scheme, &flux)) return r;
+    if (int r = check_precision_flux(c, flux)) return r;
     c->num.flux = flux;
     set_spacing(c, dx, dy);
     unsigned before = 0, after = 0;
@@ -679,6 +689,7 @@ int loop_setup(eb2_ctx* c, int order, int scheme, double dx, double dy, double t
     if (order < 1 || order > 3) return fail(EB2_EARG, "Error: Invalid time advancement method");
     int flux;
     if (int r = map_scheme(scheme, &flux)) return r;
+    if (int r = check_precision_flux(c, flux)) return r;
     c->num.flux = flux;
     set_spacing(c, dx, dy);
     double dmin = dx > dy ? dy : dx;  // min_of_two (include/function.h:58-63)

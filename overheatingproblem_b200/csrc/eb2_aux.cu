@@ -412,6 +412,9 @@ static cudaError_t riemann_dispatch(const double* ql, const double* qr, double* 
         case FLUX_HLL: k_riemann<DIR, FLUX_HLL><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
         case FLUX_HLLC: k_riemann<DIR, FLUX_HLLC><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
         case FLUX_ROE: k_riemann<DIR, FLUX_ROE><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
+        case FLUX_HLLHC: k_riemann<DIR, FLUX_HLLHC><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
+        case FLUX_HLLCHC: k_riemann<DIR, FLUX_HLLCHC><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
+        case FLUX_ROEHC: k_riemann<DIR, FLUX_ROEHC><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
         default: k_riemann<DIR, FLUX_LLF><<<nb, NT, 0, s>>>(ql, qr, f, g, gas, status); break;
     }
     return cudaGetLastError();

@@ -33,7 +33,8 @@ enum : int { BC_OUTFLOW = 0, BC_REFLECT = 1, BC_PERIODIC = 2, BC_INFLOW = 3, BC_
 
 // Riemann solvers, numbered as AR_scheme (include/CFD_convection.h:89-117).
 // Every value other than 1/2/3/11/22/33 selects the local Lax-Friedrichs flux.
-enum : int { FLUX_LLF = 0, FLUX_HLL = 1, FLUX_HLLC = 2, FLUX_ROE = 3 };
+enum : int { FLUX_LLF = 0, FLUX_HLL = 1, FLUX_HLLC = 2, FLUX_ROE = 3,
+             FLUX_HLLHC = 4, FLUX_HLLCHC = 5, FLUX_ROEHC = 6 };  // 11, 22, 33
 
 // Ideal-gas constants as the reference forms them at run time:
 // gm1 = M_gamma - 1.0, gr = M_gamma / (M_gamma - 1.0).

@@ -66,7 +66,8 @@ extern "C" int eb2_rk_step_noalloc(double* U, int nx, int ny, const eb2_noalloc_
         return fail(EB2_EARG, "recon must be 1, 2 or 5");
     if (!(cfg->gamma > 1.0)) return fail(EB2_EARG, "gamma must exceed 1");
     if (scheme == 11 || scheme == 22 || scheme == 33)
-        return fail(EB2_EUNSUPPORTED, "heat-conduction schemes are not implemented");
+        return fail(EB2_EUNSUPPORTED,
+                    "this entry point runs the classical fluxes only (not AR_scheme 11/22/33)");
     int kind[4] = {cfg->bc_left, cfg->bc_right, cfg->bc_bottom, cfg->bc_top};
     for (int s = 0; s < 4; s++) {
         if (kind[s] < BC_OUTFLOW || kind[s] > BC_FIXED) return fail(EB2_EARG, "bad bc kind");

@@ -384,12 +384,187 @@ EB2_HD void flux_llf(const double* ql, const double* qr, const Gas& g,
     for (int k = 0; k < 4; k++) F[k] = 0.5 * (FL[k] + FR[k]) - 0.5 * sp * (UR[k] - UL[k]);
 }
 
-// Riemann dispatch.  Returns false when HLL skipped the interface.
+// --- the heat-conduction ("anti-overheating") fluxes, AR_scheme 11/22/33 ---
+// Each adds to the energy flux a term proportional to the jump of the
+// specific internal energy e = p / (rho (gamma-1)) across the interface,
+// which damps the spurious wall heating of the plain solvers.
+
+// Specific internal energy e = inv_rho * p * (1/(gamma-1)), as the three
+// solvers form it (scheme.h:1966-1967, 2270-2271, 2852-2853).
+EB2_HD double specific_energy(const Side& s, double igm1) { return s.ir * s.p * igm1; }
+
+// HLLHC_Flux (include/scheme.h:1860-2136): HLL with Einfeldt speeds (sound
+// speed from gamma p / rho, eta^2 = 1/2 sqrt(rho_L rho_R) / (sum)^2 written
+// with the reciprocal sum), plus (s_L s_R / (s_R - s_L)) (e_R - e_L) rho_HLL
+// on the energy flux.  Only the y sweep falls back to the Roe sound speed when
+// the Einfeldt speed is NaN (:2085-2089; commented out in the x sweep).
+template <int DIR>
+EB2_HD void flux_hllhc(const double* ql, const double* qr, const Gas& g,
+                                           double* F) {
+    const double igm1 = 1.0 / g.gm1;
+    Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
+    double aL = sqrt(g.gamma * L.p * L.ir), aR = sqrt(g.gamma * R.p * R.ir);
+    double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+    double HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double sqL = sqrt(L.r), sqR = sqrt(R.r);
+    double ssum = sqL + sqR;
+    double isum = 1.0 / ssum;
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double Hbar = (sqL * HL + sqR * HR) * isum;
+    double eta = 0.5 * sqL * sqR * isum * isum;
+    double dun = DIR == 1 ? R.u - L.u : R.v - L.v;
+    double dd = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun);
+    if (DIR == 2 && isnan(dd)) dd = sqrt(g.gm1 * (Hbar - 0.5 * (ubar * ubar + vbar * vbar)));
+    double nbar = DIR == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    double rho_hll = (sr * R.r - sl * L.r + FL[0] - FR[0]) / (sr - sl);
+    double eL = specific_energy(L, igm1), eR = specific_energy(R, igm1);
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    } else {
+        double idiff = 1.0 / (sr - sl);
+        double slsr = sl * sr;
+        const double UL[4] = {L.r, L.ru, L.rv, L.re}, UR[4] = {R.r, R.ru, R.rv, R.re};
+        for (int k = 0; k < 4; k++)
+            F[k] = (sr * FL[k] - sl * FR[k] + slsr * (UR[k] - UL[k])) * idiff;
+        F[3] = F[3] + (slsr * idiff) * (eR - eL) * rho_hll;
+    }
+}
+
+// HLLCHC_Flux (include/scheme.h:2153-2471): HLLC with the enthalpy sound
+// speed in both sweeps and eta^2 written with a division, plus
+// (s_L s_R / (s_R - s_L)) (e_R - e_L) times the star-region density factor
+// on the energy flux of the two star states.
+template <int DIR>
+EB2_HD void flux_hllchc(const double* ql, const double* qr, const Gas& g,
+                                            double* F) {
+    const double igm1 = 1.0 / g.gm1;
+    Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
+    double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+    double HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    double aL = sqrt((g.gamma - 1.0) * (HL - 0.5 * (L.uu + L.vv)));
+    double aR = sqrt((g.gamma - 1.0) * (HR - 0.5 * (R.uu + R.vv)));
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double sqL = sqrt(L.r), sqR = sqrt(R.r);
+    double ssum = sqL + sqR;
+    double isum = 1.0 / ssum;
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double eta = 0.5 * sqL * sqR / (ssum * ssum);
+    double unL = DIR == 1 ? L.u : L.v, unR = DIR == 1 ? R.u : R.v;
+    double utL = DIR == 1 ? L.v : L.u, utR = DIR == 1 ? R.v : R.u;
+    double dun = unR - unL;
+    double dd = sqrt((sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun);
+    double nbar = DIR == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    double denom = L.r * (sl - unL) - R.r * (sr - unR);
+    double ss = (R.p - L.p + L.r * unL * (sl - unL) - R.r * unR * (sr - unR)) / denom;
+    double mL = L.r * (sl - unL) / (sl - ss);
+    double mR = R.r * (sr - unR) / (sr - ss);
+    double feL = L.re * L.ir + (ss - unL) * (ss + L.p / (L.r * (sl - unL)));
+    double feR = R.re * R.ir + (ss - unR) * (ss + R.p / (R.r * (sr - unR)));
+    double eL = specific_energy(L, igm1), eR = specific_energy(R, igm1);
+    double idiff = 1.0 / (sr - sl);
+    double slsr = sl * sr;
+    double corr = slsr * idiff * (eR - eL);
+    // normal and tangential momentum slots of the conserved order
+    const int kn = DIR == 1 ? 1 : 2, kt = DIR == 1 ? 2 : 1;
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+    } else if (sl < 0.0 && ss >= 0.0) {
+        const double UL[4] = {L.r, L.ru, L.rv, L.re};
+        F[0] = FL[0] + sl * (mL - L.r);
+        F[kn] = FL[kn] + sl * (mL * ss - UL[kn]);
+        F[kt] = FL[kt] + sl * (mL * utL - UL[kt]);
+        F[3] = FL[3] + sl * (mL * feL - L.re) + corr * mL;
+    } else if (ss < 0.0 && sr > 0.0) {
+        const double UR[4] = {R.r, R.ru, R.rv, R.re};
+        F[0] = FR[0] + sr * (mR - R.r);
+        F[kn] = FR[kn] + sr * (mR * ss - UR[kn]);
+        F[kt] = FR[kt] + sr * (mR * utR - UR[kt]);
+        F[3] = FR[3] + sr * (mR * feR - R.re) + corr * mR;
+    } else {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+    }
+}
+
+// RoeHC_Flux (include/scheme.h:2793-3109): Roe with eps = 1e-12 in the
+// 1/(2c^2) and 1/c^2 wave-strength factors, minus 1/2 |u_n + c| (e_R - e_L)
+// rho_bar on the energy flux.  Returns false where the reference skips the
+// interface (NaN Roe density, :2944-2947).
+template <int DIR>
+EB2_HD bool flux_roehc(const double* ql, const double* qr, const Gas& g,
+                                           double* F) {
+    const double igm1 = 1.0 / g.gm1;
+    const double eps = 1e-12;
+    Side L = unpack(ql, g.gm1), R = unpack(qr, g.gm1);
+    double eL = specific_energy(L, igm1), eR = specific_energy(R, igm1);
+    double HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+    double HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double sqL = sqrt(L.r), sqR = sqrt(R.r);
+    double isum = 1.0 / (sqL + sqR);
+    double rbar = sqL * sqR;
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double Hbar = (sqL * HL + sqR * HR) * isum;
+    double q2 = ubar * ubar + vbar * vbar;
+    double cbar = sqrt(g.gm1 * (Hbar - 0.5 * q2));
+    double nbar = DIR == 1 ? ubar : vbar;
+    double lam[4] = {fabs(nbar - cbar), fabs(nbar), fabs(nbar), fabs(nbar + cbar)};
+    double drho = R.r - L.r, du = R.u - L.u, dv = R.v - L.v, dp = R.p - L.p;
+    double c2 = cbar * cbar;
+    double i2c2 = 1.0 / (2.0 * c2 + eps);
+    double ic2 = 1.0 / (c2 + eps);
+    double dn = DIR == 1 ? du : dv, dtn = DIR == 1 ? dv : du;
+    double al[4];
+    al[0] = (dp - rbar * cbar * dn) * i2c2;
+    al[1] = drho - dp * ic2;
+    al[2] = rbar * dtn;
+    al[3] = (dp + rbar * cbar * dn) * i2c2;
+    double K[4][4];
+    if (DIR == 1) {
+        K[0][0] = 1.0; K[0][1] = ubar - cbar; K[0][2] = vbar; K[0][3] = Hbar - ubar * cbar;
+        K[1][0] = 1.0; K[1][1] = ubar;        K[1][2] = vbar; K[1][3] = 0.5 * q2;
+        K[2][0] = 0.0; K[2][1] = 0.0;         K[2][2] = 1.0;  K[2][3] = vbar;
+        K[3][0] = 1.0; K[3][1] = ubar + cbar; K[3][2] = vbar; K[3][3] = Hbar + ubar * cbar;
+    } else {
+        K[0][0] = 1.0; K[0][1] = ubar; K[0][2] = vbar - cbar; K[0][3] = Hbar - vbar * cbar;
+        K[1][0] = 1.0; K[1][1] = ubar; K[1][2] = vbar;        K[1][3] = 0.5 * q2;
+        K[2][0] = 0.0; K[2][1] = 1.0;  K[2][2] = 0.0;         K[2][3] = ubar;
+        K[3][0] = 1.0; K[3][1] = ubar; K[3][2] = vbar + cbar; K[3][3] = Hbar + vbar * cbar;
+    }
+    for (int c = 0; c < 4; c++) F[c] = 0.5 * (FL[c] + FR[c]);
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        double term = 0.5 * lam[w] * al[w];
+#pragma unroll
+        for (int c = 0; c < 4; c++) F[c] -= term * K[w][c];
+    }
+    if (isnan(rbar)) return false;
+    F[3] = F[3] - 0.5 * lam[3] * (eR - eL) * rbar;
+    return true;
+}
+
+// Riemann dispatch.  Returns false when HLL or RoeHC skipped the interface.
 template <int FLUX, int DIR>
 EB2_HD bool riemann(const double* ql, const double* qr, const Gas& g,
                                         double* F) {
     if (FLUX == FLUX_HLL) return flux_hll<DIR>(ql, qr, g, F);
-    if (FLUX == FLUX_HLLC) flux_hllc<DIR>(ql, qr, g, F);
+    if (FLUX == FLUX_ROEHC) return flux_roehc<DIR>(ql, qr, g, F);
+    if (FLUX == FLUX_HLLHC) flux_hllhc<DIR>(ql, qr, g, F);
+    else if (FLUX == FLUX_HLLCHC) flux_hllchc<DIR>(ql, qr, g, F);
+    else if (FLUX == FLUX_HLLC) flux_hllc<DIR>(ql, qr, g, F);
     else if (FLUX == FLUX_ROE) flux_roe<DIR>(ql, qr, g, F);
     else flux_llf<DIR>(ql, qr, g, F);
     return true;

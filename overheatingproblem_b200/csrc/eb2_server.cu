@@ -274,7 +274,8 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
     if (precision == EB2_MIXED && !characteristic)
         return fail(EB2_EUNSUPPORTED, "the mixed form reconstructs in characteristic variables");
     if (scheme == 11 || scheme == 22 || scheme == 33)
-        return fail(EB2_EUNSUPPORTED, "heat-conduction schemes are not implemented");
+        return fail(EB2_EUNSUPPORTED,
+                    "the server runs the classical fluxes only (not AR_scheme 11/22/33)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(EB2_ECUDA, "no CUDA device available; there is no CPU path");

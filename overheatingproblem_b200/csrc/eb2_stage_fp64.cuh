@@ -304,7 +304,8 @@ cudaError_t launch_flux(const StageArgs& a, cudaStream_t s) {
         case FLUX_HLL: return launch_one<RECON, CHAR, WZ, FLUX_HLL>(a, s);
         case FLUX_HLLC: return launch_one<RECON, CHAR, WZ, FLUX_HLLC>(a, s);
         case FLUX_ROE: return launch_one<RECON, CHAR, WZ, FLUX_ROE>(a, s);
-        default: return launch_one<RECON, CHAR, WZ, FLUX_LLF>(a, s);
+        case FLUX_LLF: return launch_one<RECON, CHAR, WZ, FLUX_LLF>(a, s);
+        default: return cudaErrorInvalidValue;  // the heat-conduction fluxes: eb2_stage_fp64_hc.cu
     }
 }
 

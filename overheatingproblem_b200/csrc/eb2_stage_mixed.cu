@@ -11,7 +11,8 @@ static cudaError_t by_flux(const StageArgs& a, cudaStream_t s) {
         case FLUX_HLL: return mixstage::launch_one<WZ, FLUX_HLL>(a, s);
         case FLUX_HLLC: return mixstage::launch_one<WZ, FLUX_HLLC>(a, s);
         case FLUX_ROE: return mixstage::launch_one<WZ, FLUX_ROE>(a, s);
-        default: return mixstage::launch_one<WZ, FLUX_LLF>(a, s);
+        case FLUX_LLF: return mixstage::launch_one<WZ, FLUX_LLF>(a, s);
+        default: return cudaErrorNotSupported;  // no mixed heat-conduction fluxes
     }
 }
 

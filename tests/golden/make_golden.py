@@ -29,7 +29,18 @@ GC = 4
 
 
 def save(name: str, **arrays) -> None:
-    np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+    """Write a fixture, unless the committed one already holds the same bits."""
+    path = os.path.join(OUT, name + ".npz")
+    if os.path.exists(path):
+        old = np.load(path)
+
+        def same(a, b):
+            a, b = np.atleast_1d(np.asarray(a)), np.atleast_1d(np.asarray(b))
+            return (a.shape == b.shape and a.dtype == b.dtype and
+                    np.ascontiguousarray(a).tobytes() == np.ascontiguousarray(b).tobytes())
+        if set(old.files) == set(arrays) and all(same(old[k], arrays[k]) for k in arrays):
+            return
+    np.savez_compressed(path, **arrays)
 
 
 def ref_steps(ref: Reference, p, U, steps, scheme, order=3, dmr_t=None):
@@ -63,6 +74,12 @@ def main() -> None:
         ("tvd_comp_roe_rk3", 2, 0, 1, 3, 3, ref),
         ("godunov_char_hll_rk3", 1, 1, 1, 1, 3, ref),
         ("godunov_comp_hllc_rk1", 1, 0, 1, 2, 1, ref),
+        # the heat-conduction fluxes, AR_scheme 11 / 22 / 33
+        ("charjs_hllhc_rk3", 5, 1, 0, 11, 3, wjs),
+        ("comp_weno_hllchc_rk3", 5, 0, 1, 22, 3, ref),
+        ("charz_roehc_rk3", 5, 1, 1, 33, 3, ref),
+        ("tvd_char_hllchc_rk2", 2, 1, 1, 22, 2, ref),
+        ("godunov_comp_roehc_rk1", 1, 0, 1, 33, 1, ref),
     ]
     for name, recon, ch, wz, scheme, order, lib in combos:
         p = orc.params(32, 24, recon=recon, characteristic=ch, weno_z=wz, cfl=0.5)
@@ -80,6 +97,11 @@ def main() -> None:
     n, tf = wjs.run(p, 3, 2, U, lx / 400, ly / 8, tmax, 1)
     save("wall_heating_400x8_t0.6", U0=U0, U=U, steps=n, t_final=tf)
     manifest["wall_heating_400x8_t0.6"] = f"{n} steps to t={tf}"
+    # the same run with the anti-overheating HLLCHC flux (AR_scheme 22)
+    U = U0.copy()
+    n, tf = wjs.run(p, 3, 22, U, lx / 400, ly / 8, tmax, 1)
+    save("wall_heating_400x8_t0.6_hllchc", U0=U0, U=U, steps=n, t_final=tf)
+    manifest["wall_heating_400x8_t0.6_hllchc"] = f"{n} steps to t={tf}, AR_scheme 22"
 
     # 3. double Mach reflection with the exact boundary, 48 x 12: one step of
     #    characteristic WENO5-JS + HLLC, which goes non-finite in the reference
@@ -148,7 +170,7 @@ def main() -> None:
             variant.lib.ref_recon(d, rows, cols, _ptr(Ub), _ptr(ql), _ptr(qr), dx, dy)
             out[f"ql_{tag}{d}"], out[f"qr_{tag}{d}"] = ql, qr
         ql, qr = out[f"ql_charz{d}"], out[f"qr_charz{d}"]
-        for scheme in (1, 2, 3, 4):
+        for scheme in (1, 2, 3, 4, 11, 22, 33):
             fl = np.zeros_like(U)
             lib.ref_riemann(scheme, d, rows, cols, _ptr(ql), _ptr(qr), _ptr(fl))
             out[f"flux{scheme}_{d}"] = fl

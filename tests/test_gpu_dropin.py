@@ -36,6 +36,9 @@ CASES = {
                          "Time_ADM": 1, "scheme": 3},
     "riemann2_llf_rk3": {"TestCase": "2D_Riemann_Case2", "L_nx": 40, "L_ny": 40, "scheme": 4},
     "sod_hllc_rk3": {"TestCase": "1D_Sod_Shocktube", "L_nx": 100, "L_ny": 1},
+    "riemann3_hllchc_rk3": {"TestCase": "2D_Riemann_Case3", "L_nx": 40, "L_ny": 40, "scheme": 22},
+    "riemann5_roehc_rk3": {"TestCase": "2D_Riemann_Case5", "L_nx": 36, "L_ny": 40, "scheme": 33},
+    "impactwall_hllhc_rk3": {"TestCase": "1D_Impact_Wall", "L_nx": 120, "L_ny": 1, "scheme": 11},
 }
 
 

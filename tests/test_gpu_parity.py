@@ -17,7 +17,9 @@ pytestmark = pytest.mark.gpu
 
 FQ = ["charjs_hllc_rk3", "comp_weno_hllc_rk3", "charz_roe_rk3", "charz_hll_rk2",
       "comp_weno_llf_rk1", "tvd_char_hllc_rk3", "tvd_comp_roe_rk3", "godunov_char_hll_rk3",
-      "godunov_comp_hllc_rk1"]
+      "godunov_comp_hllc_rk1",
+      "charjs_hllhc_rk3", "comp_weno_hllchc_rk3", "charz_roehc_rk3",
+      "tvd_char_hllchc_rk2", "godunov_comp_roehc_rk1"]
 
 
 def make(gpu, nx, ny, **kw):
@@ -41,14 +43,17 @@ def test_rk_steps_bit_exact(gpu, name):
     assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
 
 
-def test_wall_heating_device_loop(gpu):
+@pytest.mark.parametrize("name,scheme", [("wall_heating_400x8_t0.6", 2),
+                                         ("wall_heating_400x8_t0.6_hllchc", 22)])
+def test_wall_heating_device_loop(gpu, name, scheme):
     """The 400x8 wall-heating configuration run to t = 0.6 by the device time
-    loop (CUDA graphs): same step count, final time and bits as the reference."""
-    z = golden("wall_heating_400x8_t0.6")
+    loop (CUDA graphs): same step count, final time and bits as the reference,
+    with HLLC and with the anti-overheating HLLCHC flux."""
+    z = golden(name)
     with make(gpu, 400, 8, recon=5, characteristic=True, weno_z=False, cfl=0.5) as s:
         lx, ly, tmax = s.init_case(gpu.lib.CASE_WALL_HEATING)
         assert same_bits(s.download(), z["U0"])
-        n, tf = s.run(3, 2, lx / 400, ly / 8, tmax, n_out=1)
+        n, tf = s.run(3, scheme, lx / 400, ly / 8, tmax, n_out=1)
         U = s.download()
         assert s.status() == 0
     assert n == int(z["steps"]) and tf == float(z["t_final"])
@@ -126,7 +131,7 @@ def test_granular_operators(gpu):
                 ql, qr = s.reconstruct(d, dx, dy)
                 assert same_bits(ql[face], z[f"ql_{tag}{d}"][face]), tag
                 assert same_bits(qr[face], z[f"qr_{tag}{d}"][face]), tag
-            for scheme in (1, 2, 3, 4):
+            for scheme in (1, 2, 3, 4, 11, 22, 33):
                 fl = s.riemann(scheme, d, z[f"ql_charz{d}"], z[f"qr_charz{d}"])
                 assert same_bits(fl[face], z[f"flux{scheme}_{d}"][face]), (scheme, d)
         s.set_reconstruction(5, True, True)
@@ -223,3 +228,29 @@ def test_device_loop_matches_host_loop(gpu, oracle):
     assert (na, ta) == (nb, tb)
     assert len(seen) == 3 and abs(seen[-1][0] - 0.05) < 1e-15
     assert same_bits(interior(Ua), interior(Ub)), bit_report(interior(Ua), interior(Ub))
+
+
+def test_heat_conduction_flux_removes_the_wall_dip(gpu):
+    """AR_scheme 22 (HLLCHC) against 2 (HLLC) on the wall-heating run: the
+    density dip and temperature overshoot next to the wall disappear."""
+    prof = {}
+    for scheme in (2, 22):
+        with make(gpu, 400, 8, recon=5, characteristic=True, weno_z=False, cfl=0.5) as s:
+            lx, ly, tmax = s.init_case(gpu.lib.CASE_WALL_HEATING)
+            s.run(3, scheme, lx / 400, ly / 8, tmax)
+            pri = interior(s.con_to_pri())
+        prof[scheme] = (pri[0].mean(axis=1), (pri[3] / pri[0]).mean(axis=1))
+    rho2, T2 = prof[2]
+    rho22, T22 = prof[22]
+    plateau = np.median(rho2[10:40])
+    assert rho2[:4].min() < 0.95 * plateau          # the dip of the plain scheme
+    assert rho22[:4].min() > 0.995 * plateau        # gone with the heat-conduction flux
+    assert T22[:4].max() < T2[:4].max()
+
+
+def test_mixed_form_rejects_heat_conduction_fluxes(gpu):
+    with make(gpu, 32, 24, precision=gpu.lib.MIXED, recon=5, characteristic=True) as s:
+        s.init_case(gpu.lib.CASE_FOUR_QUADRANT)
+        with pytest.raises(gpu.EB2Error) as ei:
+            s.rk_step(3, 22, 1e-4, 1 / 32, 1 / 24)
+        assert "heat-conduction" in str(ei.value)

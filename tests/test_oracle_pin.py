@@ -16,7 +16,9 @@ from oracle.bind import (DOUBLE_MACH, FOUR_QUADRANT, INFLOW, OUTFLOW, PERIODIC, 
 
 FQ = ["charjs_hllc_rk3", "comp_weno_hllc_rk3", "charz_roe_rk3", "charz_hll_rk2",
       "comp_weno_llf_rk1", "tvd_char_hllc_rk3", "tvd_comp_roe_rk3", "godunov_char_hll_rk3",
-      "godunov_comp_hllc_rk1"]
+      "godunov_comp_hllc_rk1",
+      "charjs_hllhc_rk3", "comp_weno_hllchc_rk3", "charz_roehc_rk3",
+      "tvd_char_hllchc_rk2", "godunov_comp_roehc_rk1"]
 
 
 @pytest.mark.parametrize("name", FQ)
@@ -35,14 +37,17 @@ def test_rk_steps_match_reference(oracle, name):
     assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
 
 
-def test_wall_heating_full_run(oracle):
-    """The 400x8 wall-heating configuration to t = 0.6 (754 steps)."""
-    z = golden("wall_heating_400x8_t0.6")
+@pytest.mark.parametrize("name,scheme", [("wall_heating_400x8_t0.6", 2),
+                                         ("wall_heating_400x8_t0.6_hllchc", 22)])
+def test_wall_heating_full_run(oracle, name, scheme):
+    """The 400x8 wall-heating configuration to t = 0.6 (754 steps), with HLLC
+    and with the anti-overheating HLLCHC flux."""
+    z = golden(name)
     p = oracle.params(400, 8, recon=5, characteristic=1, weno_z=0, cfl=0.5)
     U0, lx, ly, tmax = oracle.init_case(p, WALL_HEATING)
     assert same_bits(U0, z["U0"])
     U = U0.copy()
-    n, tf = oracle.run(p, 3, 2, U, lx / 400, ly / 8, tmax, 1)
+    n, tf = oracle.run(p, 3, scheme, U, lx / 400, ly / 8, tmax, 1)
     assert n == int(z["steps"]) and tf == float(z["t_final"])
     m = noncorner_mask(U.shape)
     assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
@@ -124,7 +129,7 @@ def test_granular_operators(oracle):
             ql, qr = oracle.recon(q, d, Ub, dx, dy)
             assert same_bits(ql[face], z[f"ql_{tag}{d}"][face]), tag
             assert same_bits(qr[face], z[f"qr_{tag}{d}"][face]), tag
-        for scheme in (1, 2, 3, 4):
+        for scheme in (1, 2, 3, 4, 11, 22, 33):
             fl = oracle.riemann(p, scheme, d, z[f"ql_charz{d}"], z[f"qr_charz{d}"])
             assert same_bits(fl[face], z[f"flux{scheme}_{d}"][face]), (scheme, d)
     f, g = oracle.flux_recon(p, 2, Ub, dx, dy)
