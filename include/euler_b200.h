@@ -63,10 +63,23 @@ enum { EB2_FP64 = 0,      /* plain drop-in: bit-identical to the reference      
 enum {
     EB2_CASE_PRECISION = 0,          /* TEST_PRECISION                           */
     EB2_CASE_SOD_1D = 1,             /* TEST_1D_SHOCKTUBE                        */
+    EB2_CASE_CONTACT_1D = 2,         /* TEST_1D_CONTACTWAVE                      */
+    EB2_CASE_SHOCK_IMPACT_1D = 3,    /* TEST_1D_SHOCKIMPACT                      */
+    EB2_CASE_DOUBLE_RARE_1D = 5,     /* TEST_1D_DOUBLERARE                       */
     EB2_CASE_IMPACT_WALL_1D = 4,     /* TEST_1D_IMPACTWALL                       */
     EB2_CASE_NOH_1D = 6,             /* TEST_1D_NOHPROBLEM                       */
     EB2_CASE_RIEMANN_1 = 7,          /* TEST_2D_SHOCKTUBE_CASE1 .. CASE5 = 7..11 */
+    EB2_CASE_TAYLOR_GREEN = 12,      /* TEST_TAYLOR_GREEN_VORTEX                 */
+    EB2_CASE_GAUSSIAN_PULSE = 13,    /* TEST_GAUSSIAN_PULSE                      */
+    EB2_CASE_KELVIN_HELMHOLTZ = 14,  /* TEST_KELVIN_HELMHOLTZ                    */
+    EB2_CASE_RAYLEIGH_TAYLOR = 15,   /* TEST_RAYLEIGH_TAYLOR                     */
     EB2_CASE_DOUBLE_MACH = 16,       /* TEST_DOUBLE_MACH_REFLECTION              */
+    EB2_CASE_BLAST_WAVE = 17,        /* TEST_BLAST_WAVE                          */
+    EB2_CASE_NOH_2D = 18,            /* TEST_NOH_PROBLEM: rand() perturbations in
+                                        the order of a one-thread run           */
+    EB2_CASE_ODD_EVEN = 19,          /* TEST_OddEven_Decoupling                  */
+    EB2_CASE_BACKWARD_STEP = 20,     /* TEST_BACKWARD_STEP: the initial stream
+                                        (the step is the multi-block path)      */
     EB2_CASE_FOUR_QUADRANT = 100,    /* q[16] = (rho,u,v,p) of the upper-right,
                                         upper-left, lower-left, lower-right
                                         quadrants of [0,1]^2; q == NULL gives

@@ -203,6 +203,7 @@ class Reference:
             "ref_read_control": (None, [C.c_char_p, C.POINTER(C.c_int), _dp, C.c_char_p, i]),
             "ref_run": (C.c_long, [i, i, i, i, _dp, d, d, d, i, i, _dp]),
             "ref_num_threads": (i, []),
+            "ref_set_threads": (None, [i]),
         }
         for n_, (res, args) in sig.items():
             fn = getattr(lib, n_)

@@ -229,3 +229,4 @@ long ref_run(int order, int scheme, int rows, int cols, double *U, double dx, do
 }
 
 int ref_num_threads(void) { return omp_get_max_threads(); }
+void ref_set_threads(int n) { omp_set_num_threads(n); }

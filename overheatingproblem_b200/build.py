@@ -36,6 +36,7 @@ CUDA_SOURCES = [
     ("eb2_stage.cu", True),
     ("eb2_aux.cu", True),
     ("eb2_api.cu", True),
+    ("eb2_cases.cu", True),
     ("eb2_noalloc.cu", True),
     ("eb2_batch_fp64.cu", True),
     ("eb2_server.cu", True),

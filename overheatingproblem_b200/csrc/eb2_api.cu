@@ -397,6 +397,24 @@ int eb2::case_setup(int tc, const double* q, InitDesc& d, double* L, double& T, 
             put(1, 0.125, 0.0, 0.0, 0.1);
             T = 0.2;
             break;
+        case EB2_CASE_CONTACT_1D:  // :121-168
+            d.kind = INIT_HALF_X; d.full = 1;
+            put(0, 1.0, 0.0, 0.0, 1.0);
+            put(1, 0.125, 0.0, 0.0, 1.0);
+            T = 0.2;
+            break;
+        case EB2_CASE_SHOCK_IMPACT_1D:  // :172-219
+            d.kind = INIT_HALF_X; d.full = 1;
+            put(0, 1.0, 4.0, 0.0, 1.0);
+            put(1, 1.0, -4.0, 0.0, 1.0);
+            T = 0.2;
+            break;
+        case EB2_CASE_DOUBLE_RARE_1D:  // :223-269
+            d.kind = INIT_HALF_X; d.full = 1;
+            put(0, 1.0, -2.0, 0.0, 1.0);
+            put(1, 1.0, 2.0, 0.0, 1.0);
+            T = 0.15;
+            break;
         case EB2_CASE_IMPACT_WALL_1D:  // :273-305
             d.kind = INIT_UNIFORM; d.full = 1;
             put(0, 1.0, 1.0, 0.0, 1.0);
@@ -417,6 +435,52 @@ int eb2::case_setup(int tc, const double* q, InitDesc& d, double* L, double& T, 
             T = riemann_t[tc - 7];
             break;
         }
+        case EB2_CASE_TAYLOR_GREEN:  // :626-683
+            d.kind = INIT_FIELD;
+            L[0] = L[1] = 2.0 * M_PI;
+            T = 5.0;
+            for (int s = 0; s < 4; s++) bc[s] = BC_PERIODIC;
+            break;
+        case EB2_CASE_GAUSSIAN_PULSE:  // :684-736
+            d.kind = INIT_FIELD;
+            L[0] = L[1] = 10.0;
+            T = 4.0;
+            break;
+        case EB2_CASE_KELVIN_HELMHOLTZ:  // :737-835
+            d.kind = INIT_FIELD;
+            T = 2.0;
+            for (int s = 0; s < 4; s++) bc[s] = BC_PERIODIC;
+            break;
+        case EB2_CASE_RAYLEIGH_TAYLOR:  // :836-889
+            d.kind = INIT_FIELD;
+            L[0] = 0.25;
+            T = 1.95;
+            bc[0] = bc[1] = BC_REFLECT;
+            bc[2] = bc[3] = BC_FIXED;
+            break;
+        case EB2_CASE_BLAST_WAVE:  // :967-1060
+            d.kind = INIT_FIELD;
+            T = 0.01;
+            for (int s = 0; s < 4; s++) bc[s] = BC_REFLECT;
+            break;
+        case EB2_CASE_NOH_2D:  // :1061-1185
+            d.kind = INIT_FIELD;
+            T = 0.6;
+            for (int s = 0; s < 4; s++) bc[s] = BC_REFLECT;
+            break;
+        case EB2_CASE_ODD_EVEN:  // :1186-1296
+            d.kind = INIT_FIELD;
+            L[0] = 20.0;
+            T = 2.0;
+            bc[2] = bc[3] = BC_REFLECT;
+            break;
+        case EB2_CASE_BACKWARD_STEP:  // :1302-1388
+            d.kind = INIT_FIELD;
+            L[0] = 3.0;
+            T = 4.0;
+            bc[0] = BC_FIXED;
+            bc[2] = bc[3] = BC_REFLECT;
+            break;
         case EB2_CASE_DOUBLE_MACH:  // :890-952, boundary kinds :900-903
             d.kind = INIT_DMR;
             put(0, 8.0, 7.1447, -4.125, 116.5);
@@ -448,6 +512,7 @@ int eb2::case_setup(int tc, const double* q, InitDesc& d, double* L, double& T, 
     }
     d.lx = L[0];
     d.ly = L[1];
+    d.field_case = tc;
     return EB2_OK;
 }
 

@@ -64,6 +64,10 @@ __global__ void k_init(double* __restrict__ u, Grid g, Gas gas, InitDesc d,
                     st = yp < sqrt(3.0) * (xp - 1.0 / 6.0) ? d.st[1] : d.st[0];
                 }
                 break;
+            case INIT_FIELD:
+                // a field evaluated on the host (eb2_cases.cu), every cell
+                for (int k = 0; k < 4; k++) w[k] = column[at(k, i, j, rows, cols)];
+                break;
             case INIT_SINE:
                 // initEulerpri1D_PrecisionTest (:52-57): column GC only; the
                 // densities 1 + 0.2 sin(x) come in from the host's libm
@@ -105,7 +109,23 @@ cudaError_t launch_init(double* u, const Grid& g, const Gas& gas, const InitDesc
                         cudaStream_t s, double* pri, double* fx, double* gy) {
     const double* column = nullptr;
     double* dcol = nullptr;
-    if (d.kind == INIT_SINE) {
+    if (d.kind == INIT_FIELD) {
+        // libm (or rand) initialisers: the host evaluates the reference's
+        // expressions with the reference's C library, the GPU converts
+        size_t bytes = (size_t)4 * g.rows * g.cols * sizeof(double);
+        double* h = (double*)calloc((size_t)4 * g.rows * g.cols, sizeof(double));
+        if (!h) return cudaErrorMemoryAllocation;
+        if (!host_case_field(d.field_case, g.rows, g.cols, gas.gamma, d.lx, d.ly, h)) {
+            free(h);
+            return cudaErrorInvalidValue;
+        }
+        cudaError_t e = cudaMallocAsync(&dcol, bytes, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dcol, h, bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        free(h);
+        if (e != cudaSuccess) return e;
+        column = dcol;
+    } else if (d.kind == INIT_SINE) {
         // the sine column is evaluated with the host libm, as the reference
         // does, so the initial state matches it bit for bit
         size_t bytes = (size_t)g.nx * sizeof(double);

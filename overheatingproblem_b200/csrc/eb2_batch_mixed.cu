@@ -6,7 +6,7 @@
 namespace eb2 {
 
 template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(mixstage::NT, 3)
+__global__ void __launch_bounds__(mixstage::NT, 4)
     k_stage_batch_mixed(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
                         const int* __restrict__ nwork, int stage) {
     const int n = *nwork;

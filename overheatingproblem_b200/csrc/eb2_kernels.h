@@ -73,8 +73,15 @@ struct InitDesc {
     int full;             // fill ghosts too (the reference's 1D/Riemann cases)
     double st[4][4];      // primitive states (rho, u, v, p)
     double lx, ly;
+    int field_case;       // INIT_FIELD: the test case host_case_field evaluates
 };
-enum : int { INIT_UNIFORM = 0, INIT_HALF_X = 1, INIT_QUADRANT = 2, INIT_DMR = 3, INIT_SINE = 4 };
+enum : int { INIT_UNIFORM = 0, INIT_HALF_X = 1, INIT_QUADRANT = 2, INIT_DMR = 3, INIT_SINE = 4,
+             INIT_FIELD = 5 };
+
+// Host evaluation of the primitive field of the test cases whose reference
+// initialisers call libm or rand() (eb2_cases.cu): w[4][rows][cols], zeroed by
+// the caller.  Returns false for any other case.
+bool host_case_field(int tc, int rows, int cols, double gamma, double lx, double ly, double* w);
 
 // Initial state, domain lengths L[2], final time and boundary kinds bc[4] of
 // an EB2_CASE_* test case (eb2_api.cu).  Returns EB2_OK or an EB2_E* code.

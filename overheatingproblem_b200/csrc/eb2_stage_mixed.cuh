@@ -27,8 +27,7 @@ constexpr int YS = TX * (TY + 1);
 constexpr int NJX = (TX + 1) * TY, NJY = TX * (TY + 1);
 // FP32 tile and primitives, FP64 interface fluxes (widened exactly once, so
 // that flux differences telescope and the step conserves to FP64 round-off)
-constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS) * sizeof(float) +
-                        (size_t)(4 * XS + 4 * YS) * sizeof(double);
+constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS + 4 * XS + 4 * YS) * sizeof(float);
 
 // One interface.  s: stencil cell n = 0 of field 0 (fields FS apart, `stride`
 // along the sweep); pa/pb: primitive records of cells i and i+1 (fields PS
@@ -40,7 +39,7 @@ EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
                                                    const double* __restrict__ u, size_t ga,
                                                    size_t gb, size_t plane, float pthr,
                                                    const Gas& g, int positivity,
-                                                   double* __restrict__ out, int ostride) {
+                                                   float* __restrict__ out, int ostride) {
     const float gm1 = (float)g.gm1, gamma = (float)g.gamma;
     f32::Eig e;
     if (pa[f32::P_P * PS] < pthr || pb[f32::P_P * PS] < pthr) {
@@ -101,10 +100,10 @@ EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
     else if (FLUX == FLUX_HLL) f32::hll(L, R, gamma, F);
     else f32::llf(L, R, gamma, F);
     // (mass, normal, tangential, energy) -> (rho, rho u, rho v, rho E)
-    out[0] = (double)F[0];
-    out[ostride] = (double)(DIR == 1 ? F[1] : F[2]);
-    out[2 * ostride] = (double)(DIR == 1 ? F[2] : F[1]);
-    out[3 * ostride] = (double)F[3];
+    out[0] = F[0];
+    out[ostride] = DIR == 1 ? F[1] : F[2];
+    out[2 * ostride] = DIR == 1 ? F[2] : F[1];
+    out[3 * ostride] = F[3];
     return st;
 }
 
@@ -113,10 +112,10 @@ template <bool WZ, int FLUX>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, int tiles_x) {
     Ctrl* ctrl = a.ctrl;
     if (!ctrl->active) return;
-    extern __shared__ double smd[];
-    double* sFx = smd;
-    double* sFy = sFx + 4 * XS;
-    float* sU = reinterpret_cast<float*>(sFy + 4 * YS);
+    extern __shared__ float smf[];
+    float* sFx = smf;
+    float* sFy = sFx + 4 * XS;
+    float* sU = sFy + 4 * YS;
     float* sP = sU + 4 * FS;
     __shared__ double red[3][NT / 32];
 
@@ -191,6 +190,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
         }
 #pragma unroll
         for (int k = 0; k < 4; k++) {
+            // widened exactly; both cells of a face read the same FP32 value
             double fxp = sFx[k * XS + (rr + 1) * TY + cc], fxm = sFx[k * XS + rr * TY + cc];
             double fyp = sFy[k * YS + rr * (TY + 1) + cc + 1], fym = sFy[k * YS + rr * (TY + 1) + cc];
             double L = -(fxp - fxm) * idx - (fyp - fym) * idy + src[k];
@@ -255,7 +255,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
 
 // Single solve: one CTA per tile.
 template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(NT, 3) k_stage(StageArgs a) {
+__global__ void __launch_bounds__(NT, 4) k_stage(StageArgs a) {
     stage_tile<WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
 }
 

@@ -25,7 +25,10 @@ CASE_SOD_1D = 1
 CASE_IMPACT_WALL_1D = 4
 CASE_NOH_1D = 6
 CASE_RIEMANN = (7, 8, 9, 10, 11)
+CASE_CONTACT_1D, CASE_SHOCK_IMPACT_1D, CASE_DOUBLE_RARE_1D = 2, 3, 5
+CASE_TAYLOR_GREEN, CASE_GAUSSIAN_PULSE, CASE_KELVIN_HELMHOLTZ, CASE_RAYLEIGH_TAYLOR = 12, 13, 14, 15
 CASE_DOUBLE_MACH = 16
+CASE_BLAST_WAVE, CASE_NOH_2D, CASE_ODD_EVEN, CASE_BACKWARD_STEP = 17, 18, 19, 20
 CASE_FOUR_QUADRANT = 100
 CASE_WALL_HEATING = 101
 

@@ -69,6 +69,11 @@ class Solver:
     def set_bc(self, left, right, bottom, top):
         L.check(self._lib.eb2_set_bc(self._h, left, right, bottom, top))
 
+    def get_bc(self) -> tuple:
+        kinds = (C.c_int * 4)()
+        L.check(self._lib.eb2_get_bc(self._h, kinds))
+        return tuple(kinds)
+
     def set_bc_states(self, inflow=None, fixed=None):
         a = None if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64)
         b = None if fixed is None else np.ascontiguousarray(fixed, dtype=np.float64)

@@ -204,9 +204,14 @@ def main() -> None:
 
     # 7. the reference's own initial states (Init_Euler_2D) on 16 x 12
     inits = {}
-    for tc, (nx, ny) in {0: (16, 1), 1: (16, 12), 4: (16, 12), 6: (16, 12), 7: (16, 12),
-                         8: (16, 12), 9: (16, 12), 10: (16, 12), 11: (15, 13),
-                         16: (24, 12)}.items():
+    # one thread: the 2D Noh initialiser draws rand() inside its OpenMP loop
+    threads = ref.lib.ref_num_threads()
+    ref.lib.ref_set_threads(1)
+    for tc, (nx, ny) in {0: (16, 1), 1: (16, 12), 2: (16, 12), 3: (16, 12), 4: (16, 12),
+                         5: (16, 12), 6: (16, 12), 7: (16, 12), 8: (16, 12), 9: (16, 12),
+                         10: (16, 12), 11: (15, 13), 12: (16, 12), 13: (16, 12),
+                         14: (16, 16), 15: (8, 24), 16: (24, 12), 17: (16, 16), 18: (16, 16),
+                         19: (40, 8), 20: (24, 8)}.items():
         rows, cols = nx + 2 * GC, ny + 2 * GC
         pri = np.zeros((4, rows, cols)); U = np.zeros_like(pri)
         F = np.zeros_like(pri); G = np.zeros_like(pri)
@@ -218,8 +223,9 @@ def main() -> None:
         lib.ref_get_bc(b)
         inits[f"case{tc}"] = U
         inits[f"case{tc}_meta"] = np.array([lx.value, ly.value, tm.value] + list(b))
+    ref.lib.ref_set_threads(threads)
     save("init_cases", **inits)
-    manifest["init_cases"] = "Init_Euler_2D of the reference's cases 0,1,4,6,7-11,16"
+    manifest["init_cases"] = "Init_Euler_2D of every TestCase2D value (0-20), one thread"
 
     # 8. control files parsed by the reference's ReadControlFile
     ctl = {}

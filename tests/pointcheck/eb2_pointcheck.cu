@@ -35,8 +35,11 @@ unsigned mixed_face(const double* cells, double pthr, const Gas& g, int pos, dou
         f32::cell_prims(cells + 4 * (2 + c), g, sP + c, mixstage::PS);
         for (int k = 0; k < 4; k++) u[c + 2 * k] = cells[4 * (2 + c) + k];
     }
-    return mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, sP, sP + 1, u, 0, 1, 2, (float)pthr, g,
-                                                   pos, F, 1);
+    float Ff[4];
+    unsigned st = mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, sP, sP + 1, u, 0, 1, 2,
+                                                          (float)pthr, g, pos, Ff, 1);
+    for (int k = 0; k < 4; k++) F[k] = Ff[k];
+    return st;
 }
 
 template <int DIR, int RECON, bool CH, bool WZ>
