@@ -216,6 +216,18 @@ static double muscl(double lo, double c, double hi, double delta, int vanleer,
     return side > 0 ? c + 0.5 * s * delta : c - 0.5 * s * delta;
 }
 
+/* WENO3_L / WENO3_R, include/Reconstruction.h:1326-1400: v1..v3 = cells
+   i-1, i, i+1 (the mirror i+2, i+1, i for the right side); pow(x, 2) is x*x
+   in the reference's build */
+static double weno3(double v1, double v2, double v3) {
+    const double eps = 1e-6;
+    double s1 = (v2 - v1) * (v2 - v1), s2 = (v3 - v2) * (v3 - v2);
+    double a1 = (1.0 / 3.0) / ((eps + s1) * (eps + s1));
+    double a2 = (2.0 / 3.0) / ((eps + s2) * (eps + s2));
+    double w1 = a1 / (a1 + a2), w2 = a2 / (a1 + a2);
+    return w1 * (-0.5 * v1 + 1.5 * v2) + w2 * (0.5 * v2 + 0.5 * v3);
+}
+
 /* interface value pair from a 6-point stencil q[0..5] = cells i-2..i+3 */
 static void recon_pair(int recon, int weno_z, int vanleer, const double q[6],
                        double delta, double *qm, double *qp) {
@@ -227,6 +239,9 @@ static void recon_pair(int recon, int weno_z, int vanleer, const double q[6],
             *qm = weno5_js(q[0], q[1], q[2], q[3], q[4]);
             *qp = weno5_js(q[5], q[4], q[3], q[2], q[1]);
         }
+    } else if (recon == 3) {
+        *qm = weno3(q[1], q[2], q[3]);
+        *qp = weno3(q[4], q[3], q[2]);
     } else if (recon == 2) {
         *qm = muscl(q[1], q[2], q[3], delta, vanleer, +1);
         *qp = muscl(q[2], q[3], q[4], delta, vanleer, -1);
@@ -245,7 +260,7 @@ int orc_recon(const orc_params *p, int dir, const double *U, double *conserl,
               double *conserr, double dx, double dy) {
     const int gc = p->gc, rows = p->nx + 2 * gc, cols = p->ny + 2 * gc;
     const int recon = p->recon;
-    if (recon != 1 && recon != 2 && recon != 5) return -1;
+    if (recon != 1 && recon != 2 && recon != 3 && recon != 5) return -1;
     const int ch = p->characteristic;
     /* characteristic TVD uses van Leer, component TVD uses minmod
        (Reconstruction.h:314-315, 418-419); WENO-Z is used only by the

@@ -75,6 +75,7 @@ void ref_recon(int dir, int rows, int cols, double *U, double *ql, double *qr,
     switch (Recon_Accur) {
         case 1: Reconstruction_Godunov(dir, var, rows, cols, GhostCell, y, a, b, dx); break;
         case 2: TVD_Reconstruction(dir, var, rows, cols, GhostCell, y, a, b, dx, dy); break;
+        case 3: WENO3_Reconstruction(dir, var, rows, cols, GhostCell, y, a, b); break;
         case 5: WENO5_Reconstruction(dir, var, rows, cols, GhostCell, y, a, b); break;
         default: break;
     }

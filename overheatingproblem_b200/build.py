@@ -32,6 +32,7 @@ CUDA_SOURCES = [
     ("eb2_stage_fp64_w5.cu", True),
     ("eb2_stage_fp64_tvd.cu", True),
     ("eb2_stage_fp64_g1.cu", True),
+    ("eb2_stage_fp64_w3.cu", True),
     ("eb2_stage_fp64_hc.cu", True),
     ("eb2_stage.cu", True),
     ("eb2_aux.cu", True),

@@ -122,11 +122,16 @@ void set_spacing(eb2_ctx* c, double dx, double dy) {
     c->grid.inv_dy = 1.0 / dy;
 }
 
-// The mixed form implements the four classical fluxes only.
+// The mixed form implements characteristic WENO5 with the four classical
+// fluxes only.
 int check_precision_flux(const eb2_ctx* c, int flux) {
-    if (c->precision == EB2_MIXED && flux >= FLUX_HLLHC)
+    if (c->precision != EB2_MIXED) return EB2_OK;
+    if (flux >= FLUX_HLLHC)
         return fail(EB2_EUNSUPPORTED,
                     "the mixed form has no heat-conduction fluxes (AR_scheme 11/22/33)");
+    if (c->num.recon != 5 || !c->num.characteristic)
+        return fail(EB2_EUNSUPPORTED,
+                    "the mixed form reconstructs with characteristic WENO5 only");
     return EB2_OK;
 }
 
@@ -301,9 +306,7 @@ int eb2_set_material(eb2_ctx* c, double gamma, int source, double gravity, doubl
 
 int eb2_set_reconstruction(eb2_ctx* c, int recon, int characteristic, int weno_z) {
     if (!c) return fail(EB2_EARG, "null context");
-    if (recon == 3)
-        return fail(EB2_EUNSUPPORTED, "third-order WENO (Recon_Accur 3) is not implemented");
-    if (recon != 1 && recon != 2 && recon != 5)
+    if (recon != 1 && recon != 2 && recon != 3 && recon != 5)
         return fail(EB2_EARG,
                     "The reconstruction program with the %d-th order has not been implemented.",
                     recon);

@@ -307,8 +307,8 @@ __device__ void recon_face(const double* __restrict__ u, int i, int j, const Gri
     auto cell = [&](int k, int n) {
         return DIR == 1 ? u[at(k, i - 2 + n, j, rows, cols)] : u[at(k, i, j - 2 + n, rows, cols)];
     };
-    constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 ? 1 : 2);
-    constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 ? 5 : 4);
+    constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 || RECON == 3 ? 1 : 2);
+    constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 || RECON == 3 ? 5 : 4);
     if (!CHAR) {
         for (int k = 0; k < 4; k++) {
             double q6[6];
@@ -375,6 +375,10 @@ static cudaError_t recon_dispatch(const double* u, double* ql, double* qr, const
             if (!ch) k_recon<DIR, 5, false, false><<<nb, NT, 0, s>>>(u, ql, qr, g, gas);
             else if (wz) k_recon<DIR, 5, true, true><<<nb, NT, 0, s>>>(u, ql, qr, g, gas);
             else k_recon<DIR, 5, true, false><<<nb, NT, 0, s>>>(u, ql, qr, g, gas);
+            break;
+        case 3:
+            if (ch) k_recon<DIR, 3, true, false><<<nb, NT, 0, s>>>(u, ql, qr, g, gas);
+            else k_recon<DIR, 3, false, false><<<nb, NT, 0, s>>>(u, ql, qr, g, gas);
             break;
         case 2:
             if (ch) k_recon<DIR, 2, true, false><<<nb, NT, 0, s>>>(u, ql, qr, g, gas);

@@ -149,8 +149,23 @@ EB2_HD double muscl(double lo, double c, double hi, double delta, int side) {
     return side > 0 ? c + 0.5 * s * delta : c - 0.5 * s * delta;
 }
 
+// WENO3_L / WENO3_R (include/Reconstruction.h:1326-1400): two-point
+// smoothness, weights 1/3 and 2/3 over (1e-6 + beta)^2 (pow(x,2) is x*x in the
+// reference's build).  WENO3_L takes v1..v3 = cells i-1, i, i+1; WENO3_R the
+// mirror i+2, i+1, i.
+EB2_HD double weno3(double v1, double v2, double v3) {
+    const double eps = 1e-6;
+    double s1 = (v2 - v1) * (v2 - v1);
+    double s2 = (v3 - v2) * (v3 - v2);
+    double a1 = (1.0 / 3.0) / ((eps + s1) * (eps + s1));
+    double a2 = (2.0 / 3.0) / ((eps + s2) * (eps + s2));
+    double w1 = a1 / (a1 + a2);
+    double w2 = a2 / (a1 + a2);
+    return w1 * (-0.5 * v1 + 1.5 * v2) + w2 * (0.5 * v2 + 0.5 * v3);
+}
+
 // Interface pair (minus side, plus side) from six values q[0..5] = cells
-// i-2..i+3 of one field; RECON 5 = WENO5, 2 = TVD, 1 = first order.
+// i-2..i+3 of one field; RECON 5 = WENO5, 3 = WENO3, 2 = TVD, 1 = first order.
 template <int RECON, bool WZ, bool VANLEER>
 EB2_HD void recon_pair(const double* q, double delta, double& qm, double& qp) {
     if (RECON == 5) {
@@ -161,6 +176,9 @@ EB2_HD void recon_pair(const double* q, double delta, double& qm, double& qp) {
             qm = weno5_js(q[0], q[1], q[2], q[3], q[4]);
             qp = weno5_js(q[5], q[4], q[3], q[2], q[1]);
         }
+    } else if (RECON == 3) {
+        qm = weno3(q[1], q[2], q[3]);
+        qp = weno3(q[4], q[3], q[2]);
     } else if (RECON == 2) {
         qm = muscl<VANLEER>(q[1], q[2], q[3], delta, +1);
         qp = muscl<VANLEER>(q[2], q[3], q[4], delta, -1);

@@ -6,12 +6,14 @@ namespace eb2 {
 cudaError_t launch_stage_fp64_w5(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_fp64_tvd(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_fp64_g1(const StageArgs& a, cudaStream_t s);
+cudaError_t launch_stage_fp64_w3(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_stage_fp64_hc(const StageArgs& a, cudaStream_t s);
 
 cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s) {
     if (a.num.flux >= FLUX_HLLHC) return launch_stage_fp64_hc(a, s);
     switch (a.num.recon) {
         case 5: return launch_stage_fp64_w5(a, s);
+        case 3: return launch_stage_fp64_w3(a, s);
         case 2: return launch_stage_fp64_tvd(a, s);
         case 1: return launch_stage_fp64_g1(a, s);
         default: return cudaErrorInvalidValue;

@@ -51,8 +51,8 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
                                                    const double* __restrict__ pb, double delta,
                                                    const Gas& g, int positivity,
                                                    double* __restrict__ out, int ostride) {
-    constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 ? 1 : 2);
-    constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 ? 5 : 4);
+    constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 || RECON == 3 ? 1 : 2);
+    constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 || RECON == 3 ? 5 : 4);
     double ql[4], qr[4];
     if (CHAR) {
         double A[5], B[5];

@@ -22,6 +22,7 @@ cudaError_t launch_stage_fp64_hc(const StageArgs& a, cudaStream_t s) {
         case 5:
             if (!ch) return hc<5, false, false>(a, s);
             return a.num.weno_z ? hc<5, true, true>(a, s) : hc<5, true, false>(a, s);
+        case 3: return ch ? hc<3, true, false>(a, s) : hc<3, false, false>(a, s);
         case 2: return ch ? hc<2, true, false>(a, s) : hc<2, false, false>(a, s);
         case 1: return ch ? hc<1, true, false>(a, s) : hc<1, false, false>(a, s);
         default: return cudaErrorInvalidValue;

@@ -80,6 +80,9 @@ def main() -> None:
         ("charz_roehc_rk3", 5, 1, 1, 33, 3, ref),
         ("tvd_char_hllchc_rk2", 2, 1, 1, 22, 2, ref),
         ("godunov_comp_roehc_rk1", 1, 0, 1, 33, 1, ref),
+        # third-order WENO (Recon_Accur 3)
+        ("weno3_char_hllc_rk3", 3, 1, 1, 2, 3, ref),
+        ("weno3_comp_roe_rk2", 3, 0, 1, 3, 2, ref),
     ]
     for name, recon, ch, wz, scheme, order, lib in combos:
         p = orc.params(32, 24, recon=recon, characteristic=ch, weno_z=wz, cfl=0.5)
@@ -164,7 +167,8 @@ def main() -> None:
         out[f"eig_l{d}"], out[f"eig_r{d}"] = el, er
         for tag, (recon, ch, wz, variant) in {"charz": (5, 1, 1, ref), "charjs": (5, 1, 0, wjs),
                                               "comp": (5, 0, 1, ref), "tvdc": (2, 1, 1, ref),
-                                              "tvdm": (2, 0, 1, ref), "god": (1, 1, 1, ref)}.items():
+                                              "tvdm": (2, 0, 1, ref), "god": (1, 1, 1, ref),
+                                              "w3c": (3, 1, 1, ref), "w3m": (3, 0, 1, ref)}.items():
             variant.lib.ref_set_params(1.4, 0.5, recon, ch, 0, 1.0)
             ql = np.zeros_like(U); qr = np.zeros_like(U)
             variant.lib.ref_recon(d, rows, cols, _ptr(Ub), _ptr(ql), _ptr(qr), dx, dy)

@@ -19,7 +19,8 @@ FQ = ["charjs_hllc_rk3", "comp_weno_hllc_rk3", "charz_roe_rk3", "charz_hll_rk2",
       "comp_weno_llf_rk1", "tvd_char_hllc_rk3", "tvd_comp_roe_rk3", "godunov_char_hll_rk3",
       "godunov_comp_hllc_rk1",
       "charjs_hllhc_rk3", "comp_weno_hllchc_rk3", "charz_roehc_rk3",
-      "tvd_char_hllchc_rk2", "godunov_comp_roehc_rk1"]
+      "tvd_char_hllchc_rk2", "godunov_comp_roehc_rk1",
+      "weno3_char_hllc_rk3", "weno3_comp_roe_rk2"]
 
 
 def make(gpu, nx, ny, **kw):
@@ -126,7 +127,7 @@ def test_granular_operators(gpu):
                    (slice(None), slice(GC, -GC), slice(GC - 1, -GC))
             for tag, (recon, ch, wz) in {"charz": (5, 1, 1), "charjs": (5, 1, 0),
                                          "comp": (5, 0, 1), "tvdc": (2, 1, 1), "tvdm": (2, 0, 1),
-                                         "god": (1, 1, 1)}.items():
+                                         "god": (1, 1, 1), "w3c": (3, 1, 1), "w3m": (3, 0, 1)}.items():
                 s.set_reconstruction(recon, ch, wz)
                 ql, qr = s.reconstruct(d, dx, dy)
                 assert same_bits(ql[face], z[f"ql_{tag}{d}"][face]), tag
