@@ -351,7 +351,11 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- dist
-def dist_setup(collective=True):
+def dist_setup(collective=True, backend="nccl"):
+    """One process per GPU: rank, world size and local rank from the launcher's
+    environment; a process group (NCCL on GPUs, gloo for CPU checks) only when
+    the ranks exchange timings.  The short timeout ends ranks that wait for one
+    another with an error instead of a hang."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -360,17 +364,20 @@ def dist_setup(collective=True):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
     return world, rank, local
 
 
 def allreduce_max(x: float, world: int) -> float:
+    """Max over ranks (the whole job's device time is the slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
