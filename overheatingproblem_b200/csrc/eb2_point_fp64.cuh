@@ -8,6 +8,7 @@
 #pragma once
 
 #include "eb2_common.cuh"
+#include "eb2_fdiv.cuh"
 
 namespace eb2 {
 namespace x64 {
@@ -185,6 +186,118 @@ EB2_HD void recon_pair(const double* q, double delta, double& qm, double& qp) {
     } else {
         qm = q[2];
         qp = q[3];
+    }
+}
+
+// --- WENO weights with branch-free correctly rounded divisions ---
+// Same expressions, same order and the same bits as weno5_js, weno5_z and
+// weno3 above; each `/` becomes rcp_rn + div_rn (eb2_fdiv.cuh), sharing the
+// reciprocal where the reference divides twice by one value.  The operands
+// are recorded in a DivGuard; when it reports one outside the range in which
+// those divisions are exact, the caller recomputes with `/`.  On the host
+// these are the plain functions.
+#if defined(__CUDA_ARCH__)
+// (w1 c1) / 6 + (w2 c2) / 6 + (w3 c3) / 6 with w_k = a_k / (a1 + a2 + a3).
+// The callers' ranges give a_k > 2^-810 and a1 + a2 + a3 < 2^562, so the
+// weights are normal; the products w_k c_k are recorded as dividends.
+__device__ __forceinline__ double blend3_rn(double a1, double a2, double a3, double v1,
+                                            double v2, double v3, double v4, double v5,
+                                            DivGuard& gd) {
+    const double S = a1 + a2 + a3, yS = rcp_rn(S);
+    const double w1 = div_rn(a1, S, yS), w2 = div_rn(a2, S, yS), w3 = div_rn(a3, S, yS);
+    const double x1 = w1 * (2.0 * v1 - 7.0 * v2 + 11.0 * v3);
+    const double x2 = w2 * (-v2 + 5.0 * v3 + 2.0 * v4);
+    const double x3 = w3 * (2.0 * v3 + 5.0 * v4 - v5);
+    gd.dividend(x1);
+    gd.dividend(x2);
+    gd.dividend(x3);
+    const double y6 = 1.0 / 6.0;   // RN(1/6), folded at compile time
+    // (x_k may be -0: copysign keeps the sign `/` gives)
+    return copysign(div_rn(x1, 6.0, y6), x1) + copysign(div_rn(x2, 6.0, y6), x2) +
+           copysign(div_rn(x3, 6.0, y6), x3);
+}
+#endif
+
+// With eps + s_k in [1e-15, 2^400) (DivGuard::ok<1423>) the quotients
+// 0.1 / t / t stay in [2^-810, 2^117].
+EB2_HD double weno5_js_rn(double v1, double v2, double v3, double v4, double v5,
+                          DivGuard& gd) {
+#if defined(__CUDA_ARCH__)
+    const double eps = 1.0e-15;
+    double s1, s2, s3;
+    smooth3(v1, v2, v3, v4, v5, s1, s2, s3);
+    const double t1 = eps + s1, t2 = eps + s2, t3 = eps + s3;
+    gd.divisor(t1);
+    gd.divisor(t2);
+    gd.divisor(t3);
+    const double y1 = rcp_rn(t1), y2 = rcp_rn(t2), y3 = rcp_rn(t3);
+    const double a1 = div_rn(div_rn(0.1, t1, y1), t1, y1);
+    const double a2 = div_rn(div_rn(0.6, t2, y2), t2, y2);
+    const double a3 = div_rn(div_rn(0.3, t3, y3), t3, y3);
+    return blend3_rn(a1, a2, a3, v1, v2, v3, v4, v5, gd);
+#else
+    return weno5_js(v1, v2, v3, v4, v5);
+#endif
+}
+
+// s_k + eps in [1e-15, 2^400) and tau = |s1 - s3| zero or in [2^-500, 2^500):
+// tau / t in [2^-900, 2^560), a_k in [0.1, 2^560).
+EB2_HD double weno5_z_rn(double v1, double v2, double v3, double v4, double v5, DivGuard& gd) {
+#if defined(__CUDA_ARCH__)
+    const double eps = 1.0e-15;
+    double s1, s2, s3;
+    smooth3(v1, v2, v3, v4, v5, s1, s2, s3);
+    const double tau = fabs(s1 - s3);
+    const double t1 = s1 + eps, t2 = s2 + eps, t3 = s3 + eps;
+    gd.divisor(t1);
+    gd.divisor(t2);
+    gd.divisor(t3);
+    const unsigned ht = __double2hiint(tau);
+    gd.fine &= tau == 0.0 || ht - (523u << 20) < (1000u << 20);
+    const double a1 = 0.1 * (1.0 + div_rn(tau, t1, rcp_rn(t1)));
+    const double a2 = 0.6 * (1.0 + div_rn(tau, t2, rcp_rn(t2)));
+    const double a3 = 0.3 * (1.0 + div_rn(tau, t3, rcp_rn(t3)));
+    return blend3_rn(a1, a2, a3, v1, v2, v3, v4, v5, gd);
+#else
+    return weno5_z(v1, v2, v3, v4, v5);
+#endif
+}
+
+// (eps + s_k)^2 in [1e-12, 2^400): a_k in [2^-402, 2^40], weights normal.
+EB2_HD double weno3_rn(double v1, double v2, double v3, DivGuard& gd) {
+#if defined(__CUDA_ARCH__)
+    const double eps = 1e-6;
+    const double s1 = (v2 - v1) * (v2 - v1);
+    const double s2 = (v3 - v2) * (v3 - v2);
+    const double d1 = (eps + s1) * (eps + s1), d2 = (eps + s2) * (eps + s2);
+    gd.divisor(d1);
+    gd.divisor(d2);
+    const double a1 = div_rn(1.0 / 3.0, d1, rcp_rn(d1));
+    const double a2 = div_rn(2.0 / 3.0, d2, rcp_rn(d2));
+    const double S = a1 + a2, yS = rcp_rn(S);
+    const double w1 = div_rn(a1, S, yS), w2 = div_rn(a2, S, yS);
+    return w1 * (-0.5 * v1 + 1.5 * v2) + w2 * (0.5 * v2 + 0.5 * v3);
+#else
+    return weno3(v1, v2, v3);
+#endif
+}
+
+// recon_pair for RECON 5 and 3 through the routines above; the caller checks
+// gd.ok<1423>() and recomputes with recon_pair when it fails.
+template <int RECON, bool WZ>
+EB2_HD void recon_pair_rn(const double* q, double& qm, double& qp, DivGuard& gd) {
+    static_assert(RECON == 5 || RECON == 3, "WENO only");
+    if (RECON == 5) {
+        if (WZ) {
+            qm = weno5_z_rn(q[0], q[1], q[2], q[3], q[4], gd);
+            qp = weno5_z_rn(q[5], q[4], q[3], q[2], q[1], gd);
+        } else {
+            qm = weno5_js_rn(q[0], q[1], q[2], q[3], q[4], gd);
+            qp = weno5_js_rn(q[5], q[4], q[3], q[2], q[1], gd);
+        }
+    } else {
+        qm = weno3_rn(q[1], q[2], q[3], gd);
+        qp = weno3_rn(q[4], q[3], q[2], gd);
     }
 }
 

@@ -17,6 +17,8 @@
 // include/function.h:144-175) are reduced per block in the epilogue.
 #pragma once
 
+#include <type_traits>
+
 #include "eb2_kernels.h"
 #include "eb2_point_fp64.cuh"
 
@@ -42,26 +44,17 @@ EB2_HD bool admissible(const double* q) {
     return q[0] > 0.0 && 2.0 * q[3] * q[0] > q[1] * q[1] + q[2] * q[2];
 }
 
-// Flux at one interface.  s points at stencil cell n=0 (i-2) of field 0,
-// `stride` steps along the sweep, fields are FS apart.  pa/pb point at the
-// primitive 5-tuples of the two cells next to the interface (fields PS apart).
-template <int DIR, int RECON, bool CHAR, bool WZ, int FLUX>
-EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
-                                                   const double* __restrict__ pa,
-                                                   const double* __restrict__ pb, double delta,
-                                                   const Gas& g, int positivity,
-                                                   double* __restrict__ out, int ostride) {
+// Reconstructed states of one interface: characteristic (project on the Roe
+// left eigenvectors, reconstruct each field, project back) or per conserved
+// field.  RN selects the branch-free WENO divisions; it returns false when
+// an operand left their exact range and the caller must redo it with `/`.
+template <bool RN, int DIR, int RECON, bool CHAR, bool WZ>
+EB2_HD bool reconstruct_states(const double* __restrict__ s, int stride, const x64::Roe& e,
+                               double delta, double* ql, double* qr) {
     constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 || RECON == 3 ? 1 : 2);
     constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 || RECON == 3 ? 5 : 4);
-    double ql[4], qr[4];
+    x64::DivGuard gd;
     if (CHAR) {
-        double A[5], B[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            A[q] = pa[q * PS];
-            B[q] = pb[q * PS];
-        }
-        const x64::Roe e = x64::roe_average(A, B, g.gm1);
         double wm[4], wp[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -75,7 +68,8 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
                 for (int m = 0; m < 4; m++) acc += s[m * FS + n * stride] * l[m];
                 q6[n] = acc;
             }
-            x64::recon_pair<RECON, WZ, true>(q6, delta, wm[k], wp[k]);
+            if constexpr (RN) x64::recon_pair_rn<RECON, WZ>(q6, wm[k], wp[k], gd);
+            else x64::recon_pair<RECON, WZ, true>(q6, delta, wm[k], wp[k]);
         }
 #pragma unroll
         for (int m = 0; m < 4; m++) {
@@ -96,9 +90,42 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
             double q6[6];
 #pragma unroll
             for (int n = N0; n < N1; n++) q6[n] = s[k * FS + n * stride];
-            x64::recon_pair<RECON, false, false>(q6, delta, ql[k], qr[k]);
+            if constexpr (RN) x64::recon_pair_rn<RECON, false>(q6, ql[k], qr[k], gd);
+            else x64::recon_pair<RECON, false, false>(q6, delta, ql[k], qr[k]);
         }
     }
+    return gd.ok<1423>();
+}
+
+// Returned by interface_flux<RN = true> when a WENO operand left the range of
+// the branch-free divisions: nothing was stored, the caller redoes the
+// interface with RN = false.  Never reaches the control block.
+constexpr unsigned ST_REDO = 1u << 31;
+
+// Flux at one interface.  s points at stencil cell n=0 (i-2) of field 0,
+// `stride` steps along the sweep, fields are FS apart.  pa/pb point at the
+// primitive 5-tuples of the two cells next to the interface (fields PS apart).
+// RN: WENO weights through the branch-free divisions (RECON 5 and 3).
+template <bool RN, int DIR, int RECON, bool CHAR, bool WZ, int FLUX>
+EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
+                                                   const double* __restrict__ pa,
+                                                   const double* __restrict__ pb, double delta,
+                                                   const Gas& g, int positivity,
+                                                   double* __restrict__ out, int ostride) {
+    double ql[4], qr[4];
+    x64::Roe e{};
+    if (CHAR) {
+        double A[5], B[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            A[q] = pa[q * PS];
+            B[q] = pb[q * PS];
+        }
+        e = x64::roe_average(A, B, g.gm1);
+    }
+    constexpr bool kRN = RN && (RECON == 5 || RECON == 3);
+    if (!reconstruct_states<kRN, DIR, RECON, CHAR, WZ>(s, stride, e, delta, ql, qr))
+        return ST_REDO;
     unsigned st = 0;
     if (!(admissible(ql) && admissible(qr))) {
         if (positivity) {
@@ -163,30 +190,44 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
         __syncthreads();
     }
 
-    // 3. interface fluxes: x faces (TX+1) x TY, then y faces TX x (TY+1)
+    // 3. interface fluxes: x faces (TX+1) x TY, then y faces TX x (TY+1).
+    // A face whose WENO operands leave the range of the branch-free divisions
+    // is marked in `redo` (bit = this thread's job number) and recomputed with
+    // `/` after the pass, so the common pass carries no fallback code.
     unsigned st = 0;
     const int pos = a.num.positivity;
+    unsigned redo = 0;
+    static_assert((NJX + NJY + NT - 1) / NT <= 32, "one redo bit per job of a thread");
     // (faces that no interior cell of this tile uses -- past the domain edge in
     // a partial tile -- are skipped)
-    for (int job = threadIdx.x; job < NJX + NJY; job += NT) {
+    auto face = [&](auto rn, int job) -> unsigned {
+        constexpr bool RN = decltype(rn)::value;
         if (job < NJX) {
             int rr = job / TY, cc = job - rr * TY;
-            if (i0 - 1 + rr >= rows - GC || j0 + cc >= cols - GC) continue;
+            if (i0 - 1 + rr >= rows - GC || j0 + cc >= cols - GC) return 0u;
             const double* s = sU + rr * HY + (cc + 3);
             const double* pa = sP + rr * PY + (cc + 1);
-            st |= interface_flux<1, RECON, CHAR, WZ, FLUX>(s, HY, pa, pa + PY, a.grid.dx, g, pos,
-                                                           sFx + rr * TY + cc, XS);
-        } else {
-            int q = job - NJX;
-            int rr = q / (TY + 1), cc = q - rr * (TY + 1);
-            if (i0 + rr >= rows - GC || j0 - 1 + cc >= cols - GC) continue;
-            const double* s = sU + (rr + 3) * HY + cc;
-            const double* pa = sP + (rr + 1) * PY + cc;
-            st |= interface_flux<2, RECON, CHAR, WZ, FLUX>(s, 1, pa, pa + 1, a.grid.dy, g, pos,
-                                                           sFy + rr * (TY + 1) + cc, YS);
+            return interface_flux<RN, 1, RECON, CHAR, WZ, FLUX>(s, HY, pa, pa + PY, a.grid.dx, g,
+                                                                pos, sFx + rr * TY + cc, XS);
         }
+        int q = job - NJX;
+        int rr = q / (TY + 1), cc = q - rr * (TY + 1);
+        if (i0 + rr >= rows - GC || j0 - 1 + cc >= cols - GC) return 0u;
+        const double* s = sU + (rr + 3) * HY + cc;
+        const double* pa = sP + (rr + 1) * PY + cc;
+        return interface_flux<RN, 2, RECON, CHAR, WZ, FLUX>(s, 1, pa, pa + 1, a.grid.dy, g, pos,
+                                                            sFy + rr * (TY + 1) + cc, YS);
+    };
+    for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++) {
+        const unsigned r = face(std::true_type{}, job);
+        if (r & ST_REDO) redo |= 1u << n;
+        else st |= r;
     }
-    __syncthreads();
+    if (__syncthreads_or(redo != 0u)) {
+        for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++)
+            if (redo >> n & 1u) st |= face(std::false_type{}, job);
+        __syncthreads();
+    }
 
     // 4. flux difference, source, RK combination, wave-speed partials
     const double dt = ctrl->dt;

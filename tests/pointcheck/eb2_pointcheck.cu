@@ -21,7 +21,7 @@ unsigned fp64_face(const double* cells, double delta, const Gas& g, int pos, dou
         x64::primitive5(q[0], q[1], q[2], q[3], g, w);
         for (int k = 0; k < 5; k++) sP[k * fp64stage::PS + c] = w[k];
     }
-    return fp64stage::interface_flux<DIR, RECON, CH, WZ, FLUX>(sU, 1, sP, sP + 1, delta, g, pos,
+    return fp64stage::interface_flux<false, DIR, RECON, CH, WZ, FLUX>(sU, 1, sP, sP + 1, delta, g, pos,
                                                                F, 1);
 }
 
