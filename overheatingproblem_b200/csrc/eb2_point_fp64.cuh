@@ -38,6 +38,48 @@ EB2_HD Roe roe_average(const double* a, const double* b, double gm1) {
     return r;
 }
 
+// roe_average through the branch-free divisions (eb2_fdiv.cuh): the same
+// bits, with the operands recorded in gd; sqrt stays IEEE.  Densities and
+// c^2 are divisors ([2^-60, 2^400)), D + 1 and c small divisors (below 2^60);
+// D + 1 is near 2 - 2^-52 whenever the densities nearly agree, so its
+// reciprocal is taken with the all-ones case included.  The velocities are
+// often tiny or subnormal ahead of fronts and take div_rn_tiny.
+EB2_HD Roe roe_average_rn(const double* a, const double* b, double gm1, DivGuard& gd) {
+#if defined(__CUDA_ARCH__)
+    Roe r;
+    gd.divisor(a[0]);
+    gd.divisor(b[0]);
+    gd.reciprocal(a[0]);
+    double D = sqrt(div_rn(b[0], a[0], rcp_rn(a[0])));
+    double D1 = D + 1.0;
+    gd.small_divisor(D1);
+    const double yD = rcp_rn_any(D1);
+    const double nu = a[1] + D * b[1], nv = a[2] + D * b[2], nH = a[4] + D * b[4];
+    gd.finite(nu);
+    gd.finite(nv);
+    gd.dividend(nH);
+    r.u = copysign(div_rn_tiny(nu, D1, yD), nu);
+    r.v = copysign(div_rn_tiny(nv, D1, yD), nv);
+    r.H = copysign(div_rn(nH, D1, yD), nH);
+    r.q2 = r.u * r.u + r.v * r.v;
+    double c2 = gm1 * (r.H - 0.5 * r.q2);
+    gd.divisor(c2);
+    gd.reciprocal(c2);
+    r.c = sqrt(c2);
+    r.b1 = div_rn(gm1, c2, rcp_rn(c2));
+    r.b2 = 1.0 + r.b1 * r.q2 - r.b1 * r.H;
+    gd.small_divisor(r.c);
+    gd.reciprocal(r.c);
+    r.ic = rcp_rn(r.c);
+    r.uc = copysign(div_rn_tiny(r.u, r.c, r.ic), r.u);
+    r.vc = copysign(div_rn_tiny(r.v, r.c, r.ic), r.v);
+    return r;
+#else
+    (void)gd;
+    return roe_average(a, b, gm1);
+#endif
+}
+
 // Row k of the left-eigenvector matrix (eigen_l[k][*], Characteriz.h:346-367
 // for x, :448-469 for y).
 template <int DIR>
@@ -199,26 +241,24 @@ EB2_HD void recon_pair(const double* q, double delta, double& qm, double& qp) {
 #if defined(__CUDA_ARCH__)
 // (w1 c1) / 6 + (w2 c2) / 6 + (w3 c3) / 6 with w_k = a_k / (a1 + a2 + a3).
 // The callers' ranges give a_k > 2^-810 and a1 + a2 + a3 < 2^562, so the
-// weights are normal; the products w_k c_k are recorded as dividends.
+// weights are normal; the products w_k c_k only need to be finite.
 __device__ __forceinline__ double blend3_rn(double a1, double a2, double a3, double v1,
                                             double v2, double v3, double v4, double v5,
                                             DivGuard& gd) {
     const double S = a1 + a2 + a3, yS = rcp_rn(S);
+    gd.reciprocal(S);
     const double w1 = div_rn(a1, S, yS), w2 = div_rn(a2, S, yS), w3 = div_rn(a3, S, yS);
     const double x1 = w1 * (2.0 * v1 - 7.0 * v2 + 11.0 * v3);
     const double x2 = w2 * (-v2 + 5.0 * v3 + 2.0 * v4);
     const double x3 = w3 * (2.0 * v3 + 5.0 * v4 - v5);
-    gd.dividend(x1);
-    gd.dividend(x2);
-    gd.dividend(x3);
-    const double y6 = 1.0 / 6.0;   // RN(1/6), folded at compile time
-    // (x_k may be -0: copysign keeps the sign `/` gives)
-    return copysign(div_rn(x1, 6.0, y6), x1) + copysign(div_rn(x2, 6.0, y6), x2) +
-           copysign(div_rn(x3, 6.0, y6), x3);
+    gd.finite(x1);
+    gd.finite(x2);
+    gd.finite(x3);
+    return div6_rn(x1) + div6_rn(x2) + div6_rn(x3);
 }
 #endif
 
-// With eps + s_k in [1e-15, 2^400) (DivGuard::ok<1423>) the quotients
+// With eps + s_k in [1e-15, 2^400) (recorded divisors) the quotients
 // 0.1 / t / t stay in [2^-810, 2^117].
 EB2_HD double weno5_js_rn(double v1, double v2, double v3, double v4, double v5,
                           DivGuard& gd) {
@@ -230,6 +270,9 @@ EB2_HD double weno5_js_rn(double v1, double v2, double v3, double v4, double v5,
     gd.divisor(t1);
     gd.divisor(t2);
     gd.divisor(t3);
+    gd.reciprocal(t1);
+    gd.reciprocal(t2);
+    gd.reciprocal(t3);
     const double y1 = rcp_rn(t1), y2 = rcp_rn(t2), y3 = rcp_rn(t3);
     const double a1 = div_rn(div_rn(0.1, t1, y1), t1, y1);
     const double a2 = div_rn(div_rn(0.6, t2, y2), t2, y2);
@@ -252,6 +295,9 @@ EB2_HD double weno5_z_rn(double v1, double v2, double v3, double v4, double v5, 
     gd.divisor(t1);
     gd.divisor(t2);
     gd.divisor(t3);
+    gd.reciprocal(t1);
+    gd.reciprocal(t2);
+    gd.reciprocal(t3);
     const unsigned ht = __double2hiint(tau);
     gd.fine &= tau == 0.0 || ht - (523u << 20) < (1000u << 20);
     const double a1 = 0.1 * (1.0 + div_rn(tau, t1, rcp_rn(t1)));
@@ -272,9 +318,12 @@ EB2_HD double weno3_rn(double v1, double v2, double v3, DivGuard& gd) {
     const double d1 = (eps + s1) * (eps + s1), d2 = (eps + s2) * (eps + s2);
     gd.divisor(d1);
     gd.divisor(d2);
+    gd.reciprocal(d1);
+    gd.reciprocal(d2);
     const double a1 = div_rn(1.0 / 3.0, d1, rcp_rn(d1));
     const double a2 = div_rn(2.0 / 3.0, d2, rcp_rn(d2));
     const double S = a1 + a2, yS = rcp_rn(S);
+    gd.reciprocal(S);
     const double w1 = div_rn(a1, S, yS), w2 = div_rn(a2, S, yS);
     return w1 * (-0.5 * v1 + 1.5 * v2) + w2 * (0.5 * v2 + 0.5 * v3);
 #else
@@ -283,7 +332,7 @@ EB2_HD double weno3_rn(double v1, double v2, double v3, DivGuard& gd) {
 }
 
 // recon_pair for RECON 5 and 3 through the routines above; the caller checks
-// gd.ok<1423>() and recomputes with recon_pair when it fails.
+// gd.ok() and recomputes with recon_pair when it fails.
 template <int RECON, bool WZ>
 EB2_HD void recon_pair_rn(const double* q, double& qm, double& qp, DivGuard& gd) {
     static_assert(RECON == 5 || RECON == 3, "WENO only");

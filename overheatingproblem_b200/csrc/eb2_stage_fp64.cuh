@@ -46,14 +46,13 @@ EB2_HD bool admissible(const double* q) {
 
 // Reconstructed states of one interface: characteristic (project on the Roe
 // left eigenvectors, reconstruct each field, project back) or per conserved
-// field.  RN selects the branch-free WENO divisions; it returns false when
-// an operand left their exact range and the caller must redo it with `/`.
+// field.  RN selects the branch-free WENO divisions, whose operands are
+// recorded in gd.
 template <bool RN, int DIR, int RECON, bool CHAR, bool WZ>
-EB2_HD bool reconstruct_states(const double* __restrict__ s, int stride, const x64::Roe& e,
-                               double delta, double* ql, double* qr) {
+EB2_HD void reconstruct_states(const double* __restrict__ s, int stride, const x64::Roe& e,
+                               double delta, double* ql, double* qr, x64::DivGuard& gd) {
     constexpr int N0 = RECON == 5 ? 0 : (RECON == 2 || RECON == 3 ? 1 : 2);
     constexpr int N1 = RECON == 5 ? 6 : (RECON == 2 || RECON == 3 ? 5 : 4);
-    x64::DivGuard gd;
     if (CHAR) {
         double wm[4], wp[4];
 #pragma unroll
@@ -94,18 +93,18 @@ EB2_HD bool reconstruct_states(const double* __restrict__ s, int stride, const x
             else x64::recon_pair<RECON, false, false>(q6, delta, ql[k], qr[k]);
         }
     }
-    return gd.ok<1423>();
 }
 
-// Returned by interface_flux<RN = true> when a WENO operand left the range of
-// the branch-free divisions: nothing was stored, the caller redoes the
-// interface with RN = false.  Never reaches the control block.
+// Returned by interface_flux<RN = true> when an operand left the range of the
+// branch-free divisions: nothing was stored, the caller redoes the interface
+// with RN = false.  Never reaches the control block.
 constexpr unsigned ST_REDO = 1u << 31;
 
 // Flux at one interface.  s points at stencil cell n=0 (i-2) of field 0,
 // `stride` steps along the sweep, fields are FS apart.  pa/pb point at the
 // primitive 5-tuples of the two cells next to the interface (fields PS apart).
-// RN: WENO weights through the branch-free divisions (RECON 5 and 3).
+// RN: Roe average and WENO weights (RECON 5 and 3) through the branch-free
+// divisions.
 template <bool RN, int DIR, int RECON, bool CHAR, bool WZ, int FLUX>
 EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
                                                    const double* __restrict__ pa,
@@ -114,6 +113,7 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
                                                    double* __restrict__ out, int ostride) {
     double ql[4], qr[4];
     x64::Roe e{};
+    x64::DivGuard gd;
     if (CHAR) {
         double A[5], B[5];
 #pragma unroll
@@ -121,11 +121,11 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
             A[q] = pa[q * PS];
             B[q] = pb[q * PS];
         }
-        e = x64::roe_average(A, B, g.gm1);
+        e = RN ? x64::roe_average_rn(A, B, g.gm1, gd) : x64::roe_average(A, B, g.gm1);
     }
-    constexpr bool kRN = RN && (RECON == 5 || RECON == 3);
-    if (!reconstruct_states<kRN, DIR, RECON, CHAR, WZ>(s, stride, e, delta, ql, qr))
-        return ST_REDO;
+    constexpr bool kRNW = RN && (RECON == 5 || RECON == 3);
+    reconstruct_states<kRNW, DIR, RECON, CHAR, WZ>(s, stride, e, delta, ql, qr, gd);
+    if (RN && !gd.ok()) return ST_REDO;
     unsigned st = 0;
     if (!(admissible(ql) && admissible(qr))) {
         if (positivity) {

@@ -3,14 +3,23 @@
 // division `/` and against the routines written with `/`.
 //
 // dc_run(seed, launches, counts) runs `launches` grids of 2^22 random cases and
-// accumulates into counts[0..8]:
-//   0 rcp_rn(b) != __drcp_rn(b)              b in [2^-1000, 2^1000], all signs
-//   1 div_rn(a, b, rcp_rn(b)) != a / b       quotients in [2^-900, 2^900]
-//   2 copysign(div_rn(x, 6, RN(1/6)), x) != x / 6   x zero or in [2^-960, 2^1000]
+// accumulates into counts[0..9]:
+//   0 rcp_rn(b) != __drcp_rn(b)              b in [2^-1000, 2^1000], all signs,
+//                                            significand not all ones
+//   1 div_rn(a, b, rcp_rn(b)) != a / b       quotients in [2^-902, 2^902]
+//   2 div6_rn(x) != x / 6                    x zero, subnormal or normal, all signs
 //   3 weno5_js_rn != weno5_js where the guard holds
 //   4 weno5_z_rn  != weno5_z  where the guard holds
 //   5 weno3_rn    != weno3    where the guard holds
 //   6, 7, 8  WENO cases (JS, Z, 3) whose guard failed (recomputed with `/`)
+//   9 divisors with an all-ones significand, which DivGuard::reciprocal
+//     must report (they are left out of 0 and 1)
+//  10 roe_average_rn != roe_average (any of its ten outputs) where the
+//     guard holds, on random left/right primitive states (velocities zero of
+//     either sign, subnormal, tiny or O(1))
+//  11 Roe averages whose guard failed
+//  12 div_rn_tiny(a, b, rcp_rn_any(b)) != a / b   a zero, subnormal or below
+//     2^900, b in [2^-30, 2^60) (few-bit divisors such as 2 included)
 // Operands mix random significands with all-ones, near-zero and few-bit
 // significands; WENO stencils mix smooth data, jumps, zeros of both signs,
 // tiny and huge values, infinities and NaN.
@@ -78,16 +87,41 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
     if ((r3 >> 16) & 1) a = -a;
     if (((r3 >> 20) & 7) == 0) a = b * make(r3, 0, -2, 2);
     const double y = x64::rcp_rn(b);
-    if (!same(y, __drcp_rn(b))) atomicAdd(&counts[0], 1ull);
-    if (!same(x64::div_rn(a, b, y), a / b)) atomicAdd(&counts[1], 1ull);
+    x64::DivGuard gb;
+    gb.reciprocal(b);
+    if (gb.ok()) {
+        if (!same(y, __drcp_rn(b))) atomicAdd(&counts[0], 1ull);
+        if (!same(x64::div_rn(a, b, y), a / b)) atomicAdd(&counts[1], 1ull);
+    } else {
+        atomicAdd(&counts[9], 1ull);
+    }
     double bw = make(r4, mode_b, -1000, 1000);
     if ((r4 >> 60) & 1) bw = -bw;
-    if (!same(x64::rcp_rn(bw), __drcp_rn(bw))) atomicAdd(&counts[0], 1ull);
+    x64::DivGuard gw;
+    gw.reciprocal(bw);
+    if (gw.ok()) {
+        if (!same(x64::rcp_rn(bw), __drcp_rn(bw))) atomicAdd(&counts[0], 1ull);
+    } else {
+        atomicAdd(&counts[9], 1ull);
+    }
 
-    // division by six
-    double x = ((r4 >> 40) & 15) == 0 ? 0.0 : make(r3 ^ r1, mode_a, -960, 1000);
+    // division by six, and division of tiny dividends
+    double x;
+    const unsigned xk = (unsigned)((r4 >> 40) & 15);
+    if (xk == 0) x = 0.0;
+    else if (xk < 6) x = __longlong_as_double((long long)(r3 & 0x000fffffffffffffull) >> (r2 % 50));
+    else if (xk < 10) x = make(r3 ^ r1, mode_a, -1022, -900);
+    else x = make(r3 ^ r1, mode_a, -900, 1000);
     if ((r1 >> 60) & 1) x = -x;
-    if (!same(copysign(x64::div_rn(x, 6.0, 1.0 / 6.0), x), x / 6.0)) atomicAdd(&counts[2], 1ull);
+    if (!same(x64::div6_rn(x), x / 6.0)) atomicAdd(&counts[2], 1ull);
+    {
+        double bt = ((r4 >> 44) & 7) == 0 ? 2.0 : make(r4 ^ r2, mode_b, -30, 59);
+        const double xt = ((r4 >> 47) & 1) ? x : x * 0x1p-100;
+        if (xt < 0x1p900 && xt > -0x1p900) {
+            const double q = copysign(x64::div_rn_tiny(xt, bt, x64::rcp_rn_any(bt)), xt);
+            if (!same(q, xt / bt)) atomicAdd(&counts[12], 1ull);
+        }
+    }
 
     // WENO stencils
     double v[6];
@@ -101,7 +135,7 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
     {
         x64::DivGuard gd;
         const double f = x64::weno5_js_rn(v[0], v[1], v[2], v[3], v[4], gd);
-        if (gd.ok<1423>()) {
+        if (gd.ok()) {
             if (!same(f, x64::weno5_js(v[0], v[1], v[2], v[3], v[4]))) atomicAdd(&counts[3], 1ull);
         } else {
             atomicAdd(&counts[6], 1ull);
@@ -110,16 +144,57 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
     {
         x64::DivGuard gd;
         const double f = x64::weno5_z_rn(v[5], v[4], v[3], v[2], v[1], gd);
-        if (gd.ok<1423>()) {
+        if (gd.ok()) {
             if (!same(f, x64::weno5_z(v[5], v[4], v[3], v[2], v[1]))) atomicAdd(&counts[4], 1ull);
         } else {
             atomicAdd(&counts[7], 1ull);
         }
     }
     {
+        // primitive states (rho, u, v, p, H) of two cells, gamma 1.4
+        const double gm1 = 0.4;
+        double A[5], B[5];
+        uint64_t q = r3 ^ r4;
+        for (int c = 0; c < 2; c++) {
+            double* w = c ? B : A;
+            q = mix(q);
+            const int wide = (int)(q & 7) == 0;
+            const double rho = make(q, 0, wide ? -80 : -6, wide ? 80 : 6);
+            q = mix(q);
+            const unsigned ku = (unsigned)((q >> 3) & 7);
+            const double u = ku == 0 ? ((q & 1) ? 0.0 : -0.0)
+                           : ku == 1 ? __longlong_as_double((long long)((q >> 8) & 0xfffffffffull))
+                                         * ((q & 2) ? 1 : -1)
+                                     : make(q, 0, ku == 2 ? -1020 : -20, ku == 2 ? -900 : 4)
+                                         * ((q & 2) ? 1 : -1);
+            q = mix(q);
+            const unsigned kv = (unsigned)((q >> 3) & 7);
+            const double vv = kv == 0 ? ((q & 1) ? 0.0 : -0.0)
+                            : kv == 1 ? __longlong_as_double((long long)((q >> 8) & 0xfffffffffull))
+                                          * ((q & 2) ? 1 : -1)
+                                      : make(q, 0, kv == 2 ? -1020 : -20, kv == 2 ? -900 : 4)
+                                          * ((q & 2) ? 1 : -1);
+            q = mix(q);
+            const double p = make(q, 0, wide ? -80 : -6, wide ? 80 : 6);
+            w[0] = rho; w[1] = u; w[2] = vv; w[3] = p;
+            w[4] = (p / gm1 + 0.5 * rho * (u * u + vv * vv) + p) / rho;
+        }
+        x64::DivGuard gd;
+        const x64::Roe f = x64::roe_average_rn(A, B, gm1, gd);
+        if (gd.ok()) {
+            const x64::Roe g = x64::roe_average(A, B, gm1);
+            const bool eq = same(f.u, g.u) && same(f.v, g.v) && same(f.H, g.H) && same(f.c, g.c) &&
+                            same(f.q2, g.q2) && same(f.b1, g.b1) && same(f.b2, g.b2) &&
+                            same(f.ic, g.ic) && same(f.uc, g.uc) && same(f.vc, g.vc);
+            if (!eq) atomicAdd(&counts[10], 1ull);
+        } else {
+            atomicAdd(&counts[11], 1ull);
+        }
+    }
+    {
         x64::DivGuard gd;
         const double f = x64::weno3_rn(v[1], v[2], v[3], gd);
-        if (gd.ok<1423>()) {
+        if (gd.ok()) {
             if (!same(f, x64::weno3(v[1], v[2], v[3]))) atomicAdd(&counts[5], 1ull);
         } else {
             atomicAdd(&counts[8], 1ull);
@@ -131,13 +206,13 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
 
 extern "C" int dc_run(unsigned long long seed, int launches, unsigned long long* counts_host) {
     unsigned long long* counts = nullptr;
-    if (cudaMalloc(&counts, 9 * sizeof(unsigned long long)) != cudaSuccess) return 1;
-    cudaMemset(counts, 0, 9 * sizeof(unsigned long long));
+    if (cudaMalloc(&counts, 13 * sizeof(unsigned long long)) != cudaSuccess) return 1;
+    cudaMemset(counts, 0, 13 * sizeof(unsigned long long));
     const int threads = 256, blocks = (1 << 22) / threads;
     for (int l = 0; l < launches; l++) k_divcheck<<<blocks, threads>>>(seed + 7919ull * l, counts);
     cudaError_t err = cudaDeviceSynchronize();
     if (err == cudaSuccess)
-        err = cudaMemcpy(counts_host, counts, 9 * sizeof(unsigned long long),
+        err = cudaMemcpy(counts_host, counts, 13 * sizeof(unsigned long long),
                          cudaMemcpyDeviceToHost);
     cudaFree(counts);
     return err == cudaSuccess ? 0 : 2;

@@ -4,10 +4,11 @@ the IEEE division on the GPU.
 The FP64 stage kernels form the WENO weights with a Newton-Raphson reciprocal
 and Markstein corrections (overheatingproblem_b200/csrc/eb2_fdiv.cuh) instead
 of `/`, and fall back to `/` where an operand leaves the range in which that
-is exact.  tests/pointcheck/eb2_divcheck.cu runs random operands (all-ones,
+is exact.  tests/pointcheck/eb2_divcheck.cu runs random operands (near-all-ones,
 near-zero and few-bit significands, every exponent of the stated range) and
 random WENO stencils (jumps, signed zeros, tiny, huge, infinite, NaN and
-subnormal values) through both and counts differing bits.  The stage-level
+subnormal values) and random pairs of primitive states for the Roe average
+through both and counts differing bits.  The stage-level
 parity tests cover the same code on the reference's own data.
 """
 from __future__ import annotations
@@ -27,7 +28,8 @@ HERE = os.path.join(ROOT, "tests", "pointcheck")
 LIB = os.path.join(HERE, "libdivcheck.so")
 CSRC = os.path.join(ROOT, "overheatingproblem_b200", "csrc")
 NAMES = ["rcp_rn", "div_rn", "div by 6", "weno5_js_rn", "weno5_z_rn", "weno3_rn",
-         "js fallback", "z fallback", "w3 fallback"]
+         "js fallback", "z fallback", "w3 fallback", "all-ones divisors", "roe_average_rn",
+         "roe fallback", "div_rn_tiny"]
 
 
 @pytest.fixture(scope="module")
@@ -48,13 +50,18 @@ def dc():
 
 def test_branch_free_divisions_match_ieee(dc):
     launches = 32
-    counts = (C.c_ulonglong * 9)()
+    counts = (C.c_ulonglong * 13)()
     assert dc.dc_run(20261203, launches, counts) == 0
     got = dict(zip(NAMES, list(counts)))
     total = launches * (1 << 22)
-    for name in NAMES[:6]:
+    for name in NAMES[:6] + ["roe_average_rn", "div_rn_tiny"]:
         assert got[name] == 0, got
     # the guard sends the stencils with infinite, NaN, subnormal or huge values
     # to `/`, and only those: most random stencils stay on the fast path
-    for name in NAMES[6:]:
+    for name in NAMES[6:9]:
         assert 0 < got[name] < total // 2, got
+    # divisors with an all-ones significand (about one case in 2^18 here) are
+    # reported by the guard rather than divided
+    assert got["all-ones divisors"] > 0, got
+    # Roe averages of states with densities or c^2 outside [2^-60, 2^400)
+    assert 0 < got["roe fallback"] < total // 4, got
