@@ -253,7 +253,7 @@ int eb2_ctx_create(eb2_ctx** out, int nx, int ny, int device) {
     c->stream = c->own;
     if (cudaMalloc(&c->u, bytes) || cudaMalloc(&c->u1, bytes) || cudaMalloc(&c->u2, bytes))
         return bail(fail(EB2_ENOMEM, "device allocation of 3 x %zu bytes failed", bytes));
-    c->npartials = stage_blocks(c->grid);
+    c->npartials = stage_blocks_max(c->grid);
     if (c->npartials < 296) c->npartials = 296;
     if (cudaMalloc(&c->partials, 3 * sizeof(double) * c->npartials) ||
         cudaMalloc(&c->ctrl, sizeof(Ctrl)) || cudaMallocHost(&c->hctrl, sizeof(Ctrl)))
@@ -794,7 +794,7 @@ int loop_graph(eb2_ctx* c, int order, int per_graph, cudaGraphExec_t* out) {
         cudaGraphExecDestroy(c->gexec);
         c->gexec = nullptr;
     }
-    const int nstage = stage_blocks(c->grid);
+    const int nstage = stage_blocks(c->grid, c->precision == EB2_MIXED);
     const long long cells = (long long)c->grid.nx * c->grid.ny;
     cudaGraph_t graph = nullptr;
     long long launches0 = c->launches;
@@ -896,7 +896,7 @@ int eb2_bench_steps(eb2_ctx* c, int order, int scheme, double dx, double dy, int
     int rc = EB2_OK;
     for (int q = 0; q < nev && rc == EB2_OK; q++)
         if (cudaEventCreate(&ev[q]) != cudaSuccess) rc = fail(EB2_ECUDA, "cudaEventCreate");
-    const int nstage = stage_blocks(c->grid);
+    const int nstage = stage_blocks(c->grid, c->precision == EB2_MIXED);
     const long long cells = (long long)c->grid.nx * c->grid.ny;
     long long l0 = c->launches;
     for (int s = 0; s < nsteps && rc == EB2_OK; s++) {

@@ -34,7 +34,14 @@ void set_last_error(const char* msg);
 cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s);
 // Same contract, mixed precision (FP32 reconstruction and fluxes).
 cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s);
-int stage_blocks(const Grid& g);
+// Tile of one stage block (x rows by y columns).  FP64 form: 15 x 32 cells, so
+// that its 16 x 32 x faces and 15 x 33 y faces (1007) fill four passes of
+// 256 threads; mixed form: 16 x 32.
+constexpr int FP64_TILE_X = 15, MIXED_TILE_X = 16, STAGE_TILE_Y = 32;
+// Blocks of one stage launch of the given form, and the most of either form
+// (the size of a partials buffer).
+int stage_blocks(const Grid& g, bool mixed);
+int stage_blocks_max(const Grid& g);
 
 // Ghost-cell fill of one state at the time held in ctrl->t (or `time` when
 // ctrl is null).

@@ -10,6 +10,10 @@
 #include "eb2_common.cuh"
 #include "eb2_fdiv.cuh"
 
+#ifndef EB2_SQRT
+#define EB2_SQRT sqrt_rn
+#endif
+
 namespace eb2 {
 namespace x64 {
 
@@ -38,19 +42,20 @@ EB2_HD Roe roe_average(const double* a, const double* b, double gm1) {
     return r;
 }
 
-// roe_average through the branch-free divisions (eb2_fdiv.cuh): the same
-// bits, with the operands recorded in gd; sqrt stays IEEE.  Densities and
+// roe_average through the branch-free divisions and square roots
+// (eb2_fdiv.cuh): the same bits, with the operands recorded in gd.  Densities and
 // c^2 are divisors ([2^-60, 2^400)), D + 1 and c small divisors (below 2^60);
 // D + 1 is near 2 - 2^-52 whenever the densities nearly agree, so its
 // reciprocal is taken with the all-ones case included.  The velocities are
-// often tiny or subnormal ahead of fronts and take div_rn_tiny.
+// often tiny or subnormal ahead of fronts and take div_rn_tiny.  b[0] / a[0]
+// and c^2 are in the range of sqrt_rn.
 EB2_HD Roe roe_average_rn(const double* a, const double* b, double gm1, DivGuard& gd) {
 #if defined(__CUDA_ARCH__)
     Roe r;
     gd.divisor(a[0]);
     gd.divisor(b[0]);
     gd.reciprocal(a[0]);
-    double D = sqrt(div_rn(b[0], a[0], rcp_rn(a[0])));
+    double D = EB2_SQRT(div_rn(b[0], a[0], rcp_rn(a[0])));
     double D1 = D + 1.0;
     gd.small_divisor(D1);
     const double yD = rcp_rn_any(D1);
@@ -58,21 +63,21 @@ EB2_HD Roe roe_average_rn(const double* a, const double* b, double gm1, DivGuard
     gd.finite(nu);
     gd.finite(nv);
     gd.dividend(nH);
-    r.u = copysign(div_rn_tiny(nu, D1, yD), nu);
-    r.v = copysign(div_rn_tiny(nv, D1, yD), nv);
+    r.u = div_rn_tiny(nu, D1, yD);
+    r.v = div_rn_tiny(nv, D1, yD);
     r.H = copysign(div_rn(nH, D1, yD), nH);
     r.q2 = r.u * r.u + r.v * r.v;
     double c2 = gm1 * (r.H - 0.5 * r.q2);
     gd.divisor(c2);
     gd.reciprocal(c2);
-    r.c = sqrt(c2);
+    r.c = EB2_SQRT(c2);
     r.b1 = div_rn(gm1, c2, rcp_rn(c2));
     r.b2 = 1.0 + r.b1 * r.q2 - r.b1 * r.H;
     gd.small_divisor(r.c);
     gd.reciprocal(r.c);
     r.ic = rcp_rn(r.c);
-    r.uc = copysign(div_rn_tiny(r.u, r.c, r.ic), r.u);
-    r.vc = copysign(div_rn_tiny(r.v, r.c, r.ic), r.v);
+    r.uc = div_rn_tiny(r.u, r.c, r.ic);
+    r.vc = div_rn_tiny(r.v, r.c, r.ic);
     return r;
 #else
     (void)gd;
@@ -452,6 +457,130 @@ EB2_HD void flux_hllc(const double* ql, const double* qr, const Gas& g,
     }
 }
 
+// unpack and flux_hllc through the branch-free divisions and square roots
+// (eb2_fdiv.cuh): the same expressions and bits, the operands recorded in gd.
+// Densities and the squared sound speeds are divisors ([2^-60, 2^400)); the
+// three HLLC denominators (star-speed denominator, s_L - s_*, rho_L (s_L -
+// u_L)) are O(rho c) and recorded as small divisors; their dividends can be
+// tiny ahead of fronts and take div_rn_tiny.
+EB2_HD Side unpack_rn(const double* q, double gm1, DivGuard& gd) {
+#if defined(__CUDA_ARCH__)
+    Side s;
+    s.r = q[0]; s.ru = q[1]; s.rv = q[2]; s.re = q[3];
+    gd.divisor(s.r);
+    s.ir = rcp_rn_any(s.r);
+    s.u = s.ru * s.ir;
+    s.v = s.rv * s.ir;
+    s.uu = s.u * s.u;
+    s.vv = s.v * s.v;
+    s.p = (s.re - 0.5 * s.r * (s.uu + s.vv)) * gm1;
+    return s;
+#else
+    (void)gd;
+    return unpack(q, gm1);
+#endif
+}
+
+template <int DIR>
+EB2_HD void flux_hllc_rn(const double* ql, const double* qr, const Gas& g, double* F,
+                         DivGuard& gd) {
+#if defined(__CUDA_ARCH__)
+    Side L = unpack_rn(ql, g.gm1, gd), R = unpack_rn(qr, g.gm1, gd);
+    double HL, HR, aL, aR;
+    if (DIR == 1) {
+        HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+        HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+        const double cL = (g.gamma - 1.0) * (HL - 0.5 * (L.uu + L.vv));
+        const double cR = (g.gamma - 1.0) * (HR - 0.5 * (R.uu + R.vv));
+        gd.divisor(cL);
+        gd.divisor(cR);
+        aL = EB2_SQRT(cL);
+        aR = EB2_SQRT(cR);
+    } else {
+        const double cL = g.gamma * L.p * L.ir, cR = g.gamma * R.p * R.ir;
+        gd.divisor(cL);
+        gd.divisor(cR);
+        aL = EB2_SQRT(cL);
+        aR = EB2_SQRT(cR);
+        HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
+        HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
+    }
+    double FL[4], FR[4];
+    phys_flux<DIR>(L, HL, FL);
+    phys_flux<DIR>(R, HR, FR);
+    double unL = DIR == 1 ? L.u : L.v, unR = DIR == 1 ? R.u : R.v;
+    double sqL = EB2_SQRT(L.r), sqR = EB2_SQRT(R.r);
+    double ssum = sqL + sqR;
+    double isum = rcp_rn_any(ssum);
+    double ubar = (sqL * L.u + sqR * R.u) * isum;
+    double vbar = (sqL * L.v + sqR * R.v) * isum;
+    double eta;
+    if (DIR == 1) {
+        eta = 0.5 * sqL * sqR * isum * isum;
+    } else {
+        const double s2 = ssum * ssum;
+        eta = div_rn(0.5 * sqL * sqR, s2, rcp_rn_any(s2));
+    }
+    double dun = unR - unL;
+    const double dd2 = (sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun;
+    gd.divisor(dd2);
+    double dd = EB2_SQRT(dd2);
+    double nbar = DIR == 1 ? ubar : vbar;
+    double sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FL[k];
+        return;
+    }
+    if (sr <= 0.0) {
+        for (int k = 0; k < 4; k++) F[k] = FR[k];
+        return;
+    }
+    double denom = L.r * (sl - unL) - R.r * (sr - unR);
+    const double snum = R.p - L.p + L.r * unL * (sl - unL) - R.r * unR * (sr - unR);
+    gd.small_divisor(denom);
+    gd.finite(snum);
+    double ss = div_rn_tiny(snum, denom, rcp_rn_any(denom));
+    if (ss >= 0.0) {
+        const double mn = L.r * (sl - unL), md = sl - ss, pd = L.r * (sl - unL);
+        gd.small_divisor(md);
+        gd.small_divisor(pd);
+        gd.finite(mn);
+        gd.finite(L.p);
+        double m = div_rn_tiny(mn, md, rcp_rn_any(md));
+        double e = L.re * L.ir + (ss - unL) * (ss + div_rn_tiny(L.p, pd, rcp_rn_any(pd)));
+        F[0] = FL[0] + sl * (m - L.r);
+        if (DIR == 1) {
+            F[1] = FL[1] + sl * (m * ss - L.ru);
+            F[2] = FL[2] + sl * (m * L.v - L.rv);
+        } else {
+            F[1] = FL[1] + sl * (m * L.u - L.ru);
+            F[2] = FL[2] + sl * (m * ss - L.rv);
+        }
+        F[3] = FL[3] + sl * (m * e - L.re);
+    } else {
+        const double mn = R.r * (sr - unR), md = sr - ss, pd = R.r * (sr - unR);
+        gd.small_divisor(md);
+        gd.small_divisor(pd);
+        gd.finite(mn);
+        gd.finite(R.p);
+        double m = div_rn_tiny(mn, md, rcp_rn_any(md));
+        double e = R.re * R.ir + (ss - unR) * (ss + div_rn_tiny(R.p, pd, rcp_rn_any(pd)));
+        F[0] = FR[0] + sr * (m - R.r);
+        if (DIR == 1) {
+            F[1] = FR[1] + sr * (m * ss - R.ru);
+            F[2] = FR[2] + sr * (m * R.v - R.rv);
+        } else {
+            F[1] = FR[1] + sr * (m * R.u - R.ru);
+            F[2] = FR[2] + sr * (m * ss - R.rv);
+        }
+        F[3] = FR[3] + sr * (m * e - R.re);
+    }
+#else
+    (void)gd;
+    flux_hllc<DIR>(ql, qr, g, F);
+#endif
+}
+
 // HLL_Flux (include/scheme.h:400-674).  Returns false where the reference
 // skips the interface (`continue` on rho<=0, NaN rho, or NaN wave speed,
 // :427-436 and :500-503) and leaves its flux entry untouched.
@@ -748,6 +877,18 @@ EB2_HD bool riemann(const double* ql, const double* qr, const Gas& g,
     else if (FLUX == FLUX_ROE) flux_roe<DIR>(ql, qr, g, F);
     else flux_llf<DIR>(ql, qr, g, F);
     return true;
+}
+
+// riemann with the HLLC flux through the branch-free operations; the other
+// solvers as above.
+template <int FLUX, int DIR>
+EB2_HD bool riemann_rn(const double* ql, const double* qr, const Gas& g, double* F,
+                       DivGuard& gd) {
+    if (FLUX == FLUX_HLLC) {
+        flux_hllc_rn<DIR>(ql, qr, g, F, gd);
+        return true;
+    }
+    return riemann<FLUX, DIR>(ql, qr, g, F);
 }
 
 // Primitive state of one cell plus its enthalpy: Con_to_Pri_2D

@@ -66,7 +66,10 @@ int fail(int code, const char* fmt, ...) {
 
 size_t slot_bytes(int nx, int ny) {
     size_t n = (size_t)4 * (nx + 2 * GC) * (ny + 2 * GC) * sizeof(double);
-    int tiles = std::max(((ny + 31) / 32) * ((nx + 15) / 16), 296);
+    Grid g{};
+    g.nx = nx;
+    g.ny = ny;
+    int tiles = std::max(stage_blocks_max(g), 296);
     return 3 * n + (size_t)3 * tiles * sizeof(double);
 }
 
@@ -368,7 +371,10 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
     Slot& sl = s->slots[q];
     const int rows = r->nx + 2 * GC, cols = r->ny + 2 * GC;
     const size_t n = (size_t)4 * rows * cols * sizeof(double);
-    const int ntiles = ((r->ny + 31) / 32) * ((r->nx + 15) / 16);
+    Grid tg{};
+    tg.nx = r->nx;
+    tg.ny = r->ny;
+    const int ntiles = stage_blocks(tg, s->precision == EB2_MIXED);
     const int npart = std::max(ntiles, 296);
     CKS(cudaMallocAsync(&sl.u, n, s->stream));
     CKS(cudaMallocAsync(&sl.u1, n, s->stream));
@@ -400,7 +406,7 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
         sd.bnd.inflow[k] = mach3[k];
         for (int m = 0; m < 4; m++) sd.bnd.fixed[m][k] = mach3[k];
     }
-    sd.tiles_x = (r->ny + 31) / 32;
+    sd.tiles_x = (r->ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y;
     sd.ntiles = ntiles;
     sd.ncells = r->nx * r->ny;
     CKS(launch_init(sl.u, sd.grid, sd.gas, d, s->stream));

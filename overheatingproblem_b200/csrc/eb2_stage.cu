@@ -20,8 +20,14 @@ cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s) {
     }
 }
 
-// Upper bound of the block count of any stage kernel (partials buffer size):
-// both forms tile the interior with at least 16 x 32 cells per block.
-int stage_blocks(const Grid& g) { return ((g.ny + 31) / 32) * ((g.nx + 15) / 16); }
+int stage_blocks(const Grid& g, bool mixed) {
+    const int tx = mixed ? MIXED_TILE_X : FP64_TILE_X;
+    return ((g.ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y) * ((g.nx + tx - 1) / tx);
+}
+
+int stage_blocks_max(const Grid& g) {
+    const int a = stage_blocks(g, false), b = stage_blocks(g, true);
+    return a > b ? a : b;
+}
 
 }  // namespace eb2

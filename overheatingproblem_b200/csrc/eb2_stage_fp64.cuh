@@ -25,7 +25,7 @@
 namespace eb2 {
 namespace fp64stage {
 
-constexpr int TX = 16, TY = 32, NT = 256;
+constexpr int TX = FP64_TILE_X, TY = STAGE_TILE_Y, NT = 256;
 constexpr int HX = TX + 6, HY = TY + 6;       // U tile with halos
 constexpr int PX = TX + 2, PY = TY + 2;       // primitive region (tile + first ring)
 constexpr int FS = HX * HY;                   // field stride in sU
@@ -125,7 +125,6 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
     }
     constexpr bool kRNW = RN && (RECON == 5 || RECON == 3);
     reconstruct_states<kRNW, DIR, RECON, CHAR, WZ>(s, stride, e, delta, ql, qr, gd);
-    if (RN && !gd.ok()) return ST_REDO;
     unsigned st = 0;
     if (!(admissible(ql) && admissible(qr))) {
         if (positivity) {
@@ -139,7 +138,10 @@ EB2_HD unsigned interface_flux(const double* __restrict__ s, int stride,
         }
     }
     double F[4];
-    if (!x64::riemann<FLUX, DIR>(ql, qr, g, F)) {
+    const bool fine = RN ? x64::riemann_rn<FLUX, DIR>(ql, qr, g, F, gd)
+                         : x64::riemann<FLUX, DIR>(ql, qr, g, F);
+    if (RN && !gd.ok()) return ST_REDO;
+    if (!fine) {
         // the reference leaves a stale entry here; a NaN makes it visible
 #pragma unroll
         for (int k = 0; k < 4; k++) F[k] = nan("");

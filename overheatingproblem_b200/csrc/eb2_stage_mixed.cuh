@@ -17,7 +17,7 @@
 namespace eb2 {
 namespace mixstage {
 
-constexpr int TX = 16, TY = 32, NT = 256;
+constexpr int TX = MIXED_TILE_X, TY = STAGE_TILE_Y, NT = 256;
 constexpr int HX = TX + 6, HY = TY + 6;
 constexpr int PX = TX + 2, PY = TY + 2;
 constexpr int FS = HX * HY;

@@ -19,7 +19,9 @@
 //     either sign, subnormal, tiny or O(1))
 //  11 Roe averages whose guard failed
 //  12 div_rn_tiny(a, b, rcp_rn_any(b)) != a / b   a zero, subnormal or below
-//     2^900, b in [2^-30, 2^60) (few-bit divisors such as 2 included)
+//     2^900, |b| in [2^-30, 2^60) (few-bit divisors such as 2 included)
+//  13 sqrt_rn(x) != sqrt(x)                 x in [2^-900, 2^1000], random and
+//     squares of near-midpoints (x = RN(s nextafter(s)) and its neighbours)
 // Operands mix random significands with all-ones, near-zero and few-bit
 // significands; WENO stencils mix smooth data, jumps, zeros of both signs,
 // tiny and huge values, infinities and NaN.
@@ -116,11 +118,26 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
     if (!same(x64::div6_rn(x), x / 6.0)) atomicAdd(&counts[2], 1ull);
     {
         double bt = ((r4 >> 44) & 7) == 0 ? 2.0 : make(r4 ^ r2, mode_b, -30, 59);
+        if ((r4 >> 50) & 1) bt = -bt;
         const double xt = ((r4 >> 47) & 1) ? x : x * 0x1p-100;
         if (xt < 0x1p900 && xt > -0x1p900) {
-            const double q = copysign(x64::div_rn_tiny(xt, bt, x64::rcp_rn_any(bt)), xt);
+            const double q = x64::div_rn_tiny(xt, bt, x64::rcp_rn_any(bt));
             if (!same(q, xt / bt)) atomicAdd(&counts[12], 1ull);
         }
+    }
+
+    // square roots
+    {
+        double xs;
+        const unsigned sk = (unsigned)((r4 >> 52) & 3);
+        if (sk == 0) {
+            xs = make(r1 ^ r4, mode_a, -900, 999);
+        } else {
+            const double s0 = make(r2 ^ r4, mode_b, -440, 490);
+            const double s1 = __longlong_as_double(__double_as_longlong(s0) + 1);
+            xs = __longlong_as_double(__double_as_longlong(s0 * s1) + (long long)sk - 2);
+        }
+        if (!same(x64::sqrt_rn(xs), sqrt(xs))) atomicAdd(&counts[13], 1ull);
     }
 
     // WENO stencils
@@ -206,13 +223,13 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
 
 extern "C" int dc_run(unsigned long long seed, int launches, unsigned long long* counts_host) {
     unsigned long long* counts = nullptr;
-    if (cudaMalloc(&counts, 13 * sizeof(unsigned long long)) != cudaSuccess) return 1;
-    cudaMemset(counts, 0, 13 * sizeof(unsigned long long));
+    if (cudaMalloc(&counts, 14 * sizeof(unsigned long long)) != cudaSuccess) return 1;
+    cudaMemset(counts, 0, 14 * sizeof(unsigned long long));
     const int threads = 256, blocks = (1 << 22) / threads;
     for (int l = 0; l < launches; l++) k_divcheck<<<blocks, threads>>>(seed + 7919ull * l, counts);
     cudaError_t err = cudaDeviceSynchronize();
     if (err == cudaSuccess)
-        err = cudaMemcpy(counts_host, counts, 13 * sizeof(unsigned long long),
+        err = cudaMemcpy(counts_host, counts, 14 * sizeof(unsigned long long),
                          cudaMemcpyDeviceToHost);
     cudaFree(counts);
     return err == cudaSuccess ? 0 : 2;

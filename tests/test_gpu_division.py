@@ -1,5 +1,5 @@
-"""The branch-free FP64 divisions of the stage kernels, bit for bit against
-the IEEE division on the GPU.
+"""The branch-free FP64 divisions and square roots of the stage kernels, bit
+for bit against the IEEE operations on the GPU.
 
 The FP64 stage kernels form the WENO weights with a Newton-Raphson reciprocal
 and Markstein corrections (overheatingproblem_b200/csrc/eb2_fdiv.cuh) instead
@@ -29,7 +29,7 @@ LIB = os.path.join(HERE, "libdivcheck.so")
 CSRC = os.path.join(ROOT, "overheatingproblem_b200", "csrc")
 NAMES = ["rcp_rn", "div_rn", "div by 6", "weno5_js_rn", "weno5_z_rn", "weno3_rn",
          "js fallback", "z fallback", "w3 fallback", "all-ones divisors", "roe_average_rn",
-         "roe fallback", "div_rn_tiny"]
+         "roe fallback", "div_rn_tiny", "sqrt_rn"]
 
 
 @pytest.fixture(scope="module")
@@ -50,11 +50,11 @@ def dc():
 
 def test_branch_free_divisions_match_ieee(dc):
     launches = 32
-    counts = (C.c_ulonglong * 13)()
+    counts = (C.c_ulonglong * 14)()
     assert dc.dc_run(20261203, launches, counts) == 0
     got = dict(zip(NAMES, list(counts)))
     total = launches * (1 << 22)
-    for name in NAMES[:6] + ["roe_average_rn", "div_rn_tiny"]:
+    for name in NAMES[:6] + ["roe_average_rn", "div_rn_tiny", "sqrt_rn"]:
         assert got[name] == 0, got
     # the guard sends the stencils with infinite, NaN, subnormal or huge values
     # to `/`, and only those: most random stencils stay on the fast path
