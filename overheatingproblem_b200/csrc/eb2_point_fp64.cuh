@@ -10,10 +10,6 @@
 #include "eb2_common.cuh"
 #include "eb2_fdiv.cuh"
 
-#ifndef EB2_SQRT
-#define EB2_SQRT sqrt_rn
-#endif
-
 namespace eb2 {
 namespace x64 {
 
@@ -55,7 +51,7 @@ EB2_HD Roe roe_average_rn(const double* a, const double* b, double gm1, DivGuard
     gd.divisor(a[0]);
     gd.divisor(b[0]);
     gd.reciprocal(a[0]);
-    double D = EB2_SQRT(div_rn(b[0], a[0], rcp_rn(a[0])));
+    double D = sqrt_rn(div_rn(b[0], a[0], rcp_rn(a[0])));
     double D1 = D + 1.0;
     gd.small_divisor(D1);
     const double yD = rcp_rn_any(D1);
@@ -70,7 +66,7 @@ EB2_HD Roe roe_average_rn(const double* a, const double* b, double gm1, DivGuard
     double c2 = gm1 * (r.H - 0.5 * r.q2);
     gd.divisor(c2);
     gd.reciprocal(c2);
-    r.c = EB2_SQRT(c2);
+    r.c = sqrt_rn(c2);
     r.b1 = div_rn(gm1, c2, rcp_rn(c2));
     r.b2 = 1.0 + r.b1 * r.q2 - r.b1 * r.H;
     gd.small_divisor(r.c);
@@ -494,14 +490,14 @@ EB2_HD void flux_hllc_rn(const double* ql, const double* qr, const Gas& g, doubl
         const double cR = (g.gamma - 1.0) * (HR - 0.5 * (R.uu + R.vv));
         gd.divisor(cL);
         gd.divisor(cR);
-        aL = EB2_SQRT(cL);
-        aR = EB2_SQRT(cR);
+        aL = sqrt_rn(cL);
+        aR = sqrt_rn(cR);
     } else {
         const double cL = g.gamma * L.p * L.ir, cR = g.gamma * R.p * R.ir;
         gd.divisor(cL);
         gd.divisor(cR);
-        aL = EB2_SQRT(cL);
-        aR = EB2_SQRT(cR);
+        aL = sqrt_rn(cL);
+        aR = sqrt_rn(cR);
         HL = 0.5 * (L.uu + L.vv) + g.gr * (L.p * L.ir);
         HR = 0.5 * (R.uu + R.vv) + g.gr * (R.p * R.ir);
     }
@@ -509,7 +505,7 @@ EB2_HD void flux_hllc_rn(const double* ql, const double* qr, const Gas& g, doubl
     phys_flux<DIR>(L, HL, FL);
     phys_flux<DIR>(R, HR, FR);
     double unL = DIR == 1 ? L.u : L.v, unR = DIR == 1 ? R.u : R.v;
-    double sqL = EB2_SQRT(L.r), sqR = EB2_SQRT(R.r);
+    double sqL = sqrt_rn(L.r), sqR = sqrt_rn(R.r);
     double ssum = sqL + sqR;
     double isum = rcp_rn_any(ssum);
     double ubar = (sqL * L.u + sqR * R.u) * isum;
@@ -524,7 +520,7 @@ EB2_HD void flux_hllc_rn(const double* ql, const double* qr, const Gas& g, doubl
     double dun = unR - unL;
     const double dd2 = (sqL * aL * aL + sqR * aR * aR) * isum + eta * dun * dun;
     gd.divisor(dd2);
-    double dd = EB2_SQRT(dd2);
+    double dd = sqrt_rn(dd2);
     double nbar = DIR == 1 ? ubar : vbar;
     double sl = nbar - dd, sr = nbar + dd;
     if (sl >= 0.0) {
