@@ -19,7 +19,8 @@
 //     either sign, subnormal, tiny or O(1))
 //  11 Roe averages whose guard failed
 //  12 div_rn_tiny(a, b, rcp_rn_any(b)) != a / b   a zero, subnormal or below
-//     2^900, |b| in [2^-30, 2^60) (few-bit divisors such as 2 included)
+//     2^900, |b| in [2^-30, 2^60) (few-bit divisors such as 2 included;
+//     quotients at the subnormal/normal boundary included)
 //  13 sqrt_rn(x) != sqrt(x)                 x in [2^-900, 2^1000], random and
 //     squares of near-midpoints (x = RN(s nextafter(s)) and its neighbours)
 // Operands mix random significands with all-ones, near-zero and few-bit
@@ -119,7 +120,10 @@ __global__ void k_divcheck(uint64_t seed, unsigned long long* counts) {
     {
         double bt = ((r4 >> 44) & 7) == 0 ? 2.0 : make(r4 ^ r2, mode_b, -30, 59);
         if ((r4 >> 50) & 1) bt = -bt;
-        const double xt = ((r4 >> 47) & 1) ? x : x * 0x1p-100;
+        double xt = ((r4 >> 47) & 1) ? x : x * 0x1p-100;
+        // quotients at the subnormal/normal boundary: a = (2^-1022 (1 + e)) b
+        if (((r4 >> 53) & 7) == 0)
+            xt = 0x1p-1022 * (1.0 + (double)((int)(r1 & 0xff) - 128) * 0x1p-52) * bt;
         if (xt < 0x1p900 && xt > -0x1p900) {
             const double q = x64::div_rn_tiny(xt, bt, x64::rcp_rn_any(bt));
             if (!same(q, xt / bt)) atomicAdd(&counts[12], 1ull);

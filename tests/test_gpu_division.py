@@ -49,7 +49,8 @@ def dc():
 
 
 def test_branch_free_divisions_match_ieee(dc):
-    launches = 32
+    # 2^22 cases per launch; EB2_DIVCHECK_LAUNCHES=512 runs 2.1e9 (about 10 s)
+    launches = int(os.environ.get("EB2_DIVCHECK_LAUNCHES", "32"))
     counts = (C.c_ulonglong * 14)()
     assert dc.dc_run(20261203, launches, counts) == 0
     got = dict(zip(NAMES, list(counts)))
