@@ -293,6 +293,35 @@ def measured_traffic(nx, precision, scheme):
     return None
 
 
+def measured_compute(precision):
+    """The binding on-chip limit of the stage kernel, from the committed ncu
+    summary profiles/stage_<precision>_2048.md (its "now" column): FP64 pipe
+    activity for the FP64 form, issue activity for the mixed form (fractions
+    of peak), or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        f"stage_{precision}_2048.md")
+    row = "FP64 pipe active" if precision == "fp64" else "issue active"
+    if not os.path.exists(path):
+        return None
+    col = None
+    for line in open(path):
+        if not line.startswith("|"):
+            continue
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if cells[0] == "metric":
+            col = next((i for i, c in enumerate(cells) if c.startswith("now") or "(now)" in c),
+                       None)
+        elif col is not None and cells[0].startswith(row) and len(cells) > col:
+            try:
+                frac = float(cells[col].split()[0]) / 100.0
+            except ValueError:
+                return None
+            return {"limit": "fp64 pipe" if precision == "fp64" else "instruction issue",
+                    "active_frac": frac,
+                    "source": f"profiles/stage_{precision}_2048.md (ncu, 2048^2 stage)"}
+    return None
+
+
 def hbm_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -499,7 +528,8 @@ def run_ours(args, world, rank, local):
                 "kernel": f"eb2 fused x+y sweep + RK stage ({args.precision})",
                 "per_launch_ms": stage_ms / nstage, "peak_kind": peak_kind,
                 "alg_bytes_per_launch": nx * nx * BYTES_PER_CELL_STEP / ORDER,
-                "stage_share_of_step": stage_ms / sum(step_ms)}
+                "stage_share_of_step": stage_ms / sum(step_ms),
+                "compute": measured_compute(args.precision)}
 
     e2e = None
     if not args.no_e2e:
