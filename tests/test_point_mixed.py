@@ -27,9 +27,11 @@ def pc():
     newest = max(os.path.getmtime(os.path.join(CSRC, f)) for f in os.listdir(CSRC))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(newest, os.path.getmtime(src)):
         nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+        # host functions only: embed PTX and skip ptxas, which would take minutes
+        # for the stage templates the header pulls in
         subprocess.run([nvcc, "-O2", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-                        "-gencode", "arch=compute_100a,code=sm_100a", "-I", CSRC, src, "-o",
-                        LIB], check=True, capture_output=True)
+                        "-gencode", "arch=compute_100a,code=compute_100a", "-I", CSRC, src,
+                        "-o", LIB], check=True, capture_output=True)
     lib = C.CDLL(LIB)
     dp = C.POINTER(C.c_double)
     lib.pc_face_fp64.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, dp, C.c_double, C.c_int, dp]
