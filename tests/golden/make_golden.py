@@ -106,6 +106,29 @@ def main() -> None:
     save("wall_heating_400x8_t0.6_hllchc", U0=U0, U=U, steps=n, t_final=tf)
     manifest["wall_heating_400x8_t0.6_hllchc"] = f"{n} steps to t={tf}, AR_scheme 22"
 
+    # 2b. Rayleigh-Taylor (TestCase2D 15) on 16 x 64 from the reference's own
+    #     Init_Euler_2D state and boundary kinds (reflecting sides, fixed-value
+    #     bottom and top), gravity source on (Gravity 1.0, the control-file
+    #     default), characteristic WENO5 as shipped + HLLC + SSP-RK3, CFL 0.5,
+    #     run by the reference's time loop to t = 0.5
+    nx, ny = 16, 64
+    rows, cols = nx + 2 * GC, ny + 2 * GC
+    pri = np.zeros((4, rows, cols)); U = np.zeros_like(pri)
+    F = np.zeros_like(pri); G = np.zeros_like(pri)
+    lx, ly, tm = C.c_double(), C.c_double(), C.c_double()
+    ref.lib.ref_set_params(1.4, 0.5, 5, 1, 1, 1.0)
+    ref.lib.ref_init(15, rows, cols, _ptr(pri), _ptr(U), _ptr(F), _ptr(G), C.byref(lx),
+                     C.byref(ly), C.byref(tm))
+    b = (C.c_int * 4)()
+    ref.lib.ref_get_bc(b)
+    U0 = U.copy()
+    tf = C.c_double()
+    n = ref.lib.ref_run(3, 2, rows, cols, _ptr(U), lx.value / nx, ly.value / ny, 0.5, 1, 0,
+                        C.byref(tf))
+    save("rayleigh_taylor_16x64_t0.5", U0=U0, U=U, steps=n, t_final=tf.value,
+         lx=lx.value, ly=ly.value, bc=np.array(list(b)))
+    manifest["rayleigh_taylor_16x64_t0.5"] = f"{n} steps to t={tf.value}, gravity source"
+
     # 3. double Mach reflection with the exact boundary, 48 x 12: one step of
     #    characteristic WENO5-JS + HLLC, which goes non-finite in the reference
     #    (negative interface pressure at the wall next to the shock foot).  HLL

@@ -62,6 +62,29 @@ def test_wall_heating_device_loop(gpu, name, scheme):
     assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
 
 
+def test_rayleigh_taylor_device_loop(gpu):
+    """Rayleigh-Taylor (TestCase2D 15), 16x64 to t = 0.5 by the device time
+    loop: the case's own initial state and boundaries (reflecting sides,
+    fixed-value bottom and top), the gravity source, characteristic WENO5 with
+    the reference's default WENO-Z weights + HLLC; same step count, final time
+    and bits as the reference."""
+    z = golden("rayleigh_taylor_16x64_t0.5")
+    with make(gpu, 16, 64, recon=5, characteristic=True, weno_z=True, cfl=0.5, source=True,
+              gravity=1.0) as s:
+        lx, ly, _ = s.init_case(gpu.lib.CASE_RAYLEIGH_TAYLOR)
+        assert (lx, ly) == (float(z["lx"]), float(z["ly"]))
+        assert tuple(s.get_bc()) == tuple(int(b) for b in z["bc"])
+        U0 = s.download()
+        assert same_bits(interior(U0), interior(z["U0"]))
+        s.upload(z["U0"])
+        n, tf = s.run(3, 2, lx / 16, ly / 64, 0.5, n_out=1)
+        U = s.download()
+        assert s.status() == 0
+    assert n == int(z["steps"]) and tf == float(z["t_final"])
+    m = noncorner_mask(U.shape)
+    assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
+
+
 def test_double_mach_nonfinite_onset(gpu):
     """The exact double-Mach boundary goes non-finite on the first step in the
     reference; the GPU reproduces the same cells and flags it."""

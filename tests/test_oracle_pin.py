@@ -11,8 +11,8 @@ import numpy as np
 import pytest
 
 from conftest import GC, bit_report, golden, interior, noncorner_mask, same_bits
-from oracle.bind import (DOUBLE_MACH, FOUR_QUADRANT, INFLOW, OUTFLOW, PERIODIC, REFLECT,
-                         WALL_HEATING, Reference)
+from oracle.bind import (DOUBLE_MACH, FIXED, FOUR_QUADRANT, INFLOW, OUTFLOW, PERIODIC,
+                         REFLECT, WALL_HEATING, Reference)
 
 FQ = ["charjs_hllc_rk3", "comp_weno_hllc_rk3", "charz_roe_rk3", "charz_hll_rk2",
       "comp_weno_llf_rk1", "tvd_char_hllc_rk3", "tvd_comp_roe_rk3", "godunov_char_hll_rk3",
@@ -49,6 +49,23 @@ def test_wall_heating_full_run(oracle, name, scheme):
     assert same_bits(U0, z["U0"])
     U = U0.copy()
     n, tf = oracle.run(p, 3, scheme, U, lx / 400, ly / 8, tmax, 1)
+    assert n == int(z["steps"]) and tf == float(z["t_final"])
+    m = noncorner_mask(U.shape)
+    assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
+
+
+def test_rayleigh_taylor_full_run(oracle):
+    """Rayleigh-Taylor (TestCase2D 15), 16x64 to t = 0.5 (254 steps): the
+    gravity source and the fixed-value bottom and top boundaries (the Mach-3
+    state the reference's globals hold) in a full time loop, started from the
+    reference's own initial state."""
+    z = golden("rayleigh_taylor_16x64_t0.5")
+    bc = tuple(int(b) for b in z["bc"])
+    assert bc == (REFLECT, REFLECT, FIXED, FIXED)
+    p = oracle.params(16, 64, recon=5, characteristic=1, weno_z=1, cfl=0.5, source=1,
+                      gravity=1.0, bc=bc)
+    U = z["U0"].copy()
+    n, tf = oracle.run(p, 3, 2, U, float(z["lx"]) / 16, float(z["ly"]) / 64, 0.5, 1)
     assert n == int(z["steps"]) and tf == float(z["t_final"])
     m = noncorner_mask(U.shape)
     assert same_bits(U[:, m], z["U"][:, m]), bit_report(U[:, m], z["U"][:, m])
