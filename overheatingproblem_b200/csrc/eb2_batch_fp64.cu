@@ -47,6 +47,9 @@ static cudaError_t by_flux(const BatchLaunch& b, int flux, int stage, cudaStream
         case FLUX_HLL: return one<RECON, CHAR, WZ, FLUX_HLL>(b, stage, s);
         case FLUX_HLLC: return one<RECON, CHAR, WZ, FLUX_HLLC>(b, stage, s);
         case FLUX_ROE: return one<RECON, CHAR, WZ, FLUX_ROE>(b, stage, s);
+        case FLUX_HLLHC: return one<RECON, CHAR, WZ, FLUX_HLLHC>(b, stage, s);
+        case FLUX_HLLCHC: return one<RECON, CHAR, WZ, FLUX_HLLCHC>(b, stage, s);
+        case FLUX_ROEHC: return one<RECON, CHAR, WZ, FLUX_ROEHC>(b, stage, s);
         default: return one<RECON, CHAR, WZ, FLUX_LLF>(b, stage, s);
     }
 }

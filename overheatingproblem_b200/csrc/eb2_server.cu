@@ -276,9 +276,9 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
     if (recon != 5) return fail(EB2_EUNSUPPORTED, "the server runs WENO5 reconstructions");
     if (precision == EB2_MIXED && !characteristic)
         return fail(EB2_EUNSUPPORTED, "the mixed form reconstructs in characteristic variables");
-    if (scheme == 11 || scheme == 22 || scheme == 33)
+    if (precision == EB2_MIXED && (scheme == 11 || scheme == 22 || scheme == 33))
         return fail(EB2_EUNSUPPORTED,
-                    "the server runs the classical fluxes only (not AR_scheme 11/22/33)");
+                    "the mixed form runs the classical fluxes only (not AR_scheme 11/22/33)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(EB2_ECUDA, "no CUDA device available; there is no CPU path");
@@ -291,7 +291,13 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
     s->num.recon = recon;
     s->num.characteristic = characteristic ? 1 : 0;
     s->num.weno_z = weno_z ? 1 : 0;
-    s->num.flux = scheme == 1 ? FLUX_HLL : scheme == 2 ? FLUX_HLLC : scheme == 3 ? FLUX_ROE : FLUX_LLF;
+    s->num.flux = scheme == 1    ? FLUX_HLL
+                  : scheme == 2  ? FLUX_HLLC
+                  : scheme == 3  ? FLUX_ROE
+                  : scheme == 11 ? FLUX_HLLHC
+                  : scheme == 22 ? FLUX_HLLCHC
+                  : scheme == 33 ? FLUX_ROEHC
+                                 : FLUX_LLF;
     s->gamma = gamma;
     s->budget = hbm_budget_bytes;
     s->nslots = max_slots;

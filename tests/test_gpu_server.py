@@ -37,7 +37,7 @@ def mix(gpu):
     return reqs
 
 
-def run_alone_ctx(gpu, req, precision):
+def run_alone_ctx(gpu, req, precision, scheme=2):
     """The same solve on a single-solve context (eb2_run)."""
     with gpu.Solver(req.nx, req.ny, precision=precision, recon=5, characteristic=True,
                     weno_z=False, cfl=req.cfl) as s:
@@ -46,21 +46,22 @@ def run_alone_ctx(gpu, req, precision):
             ly = req.ly
         if req.lx > 0:
             lx = req.lx
-        s.run(3, 2, lx / req.nx, ly / req.ny, req.tmax)
+        s.run(3, scheme, lx / req.nx, ly / req.ny, req.tmax)
         return s.download()
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_result_same_alone_and_in_the_mix(gpu, precision):
+# (the FP64 form also with the anti-overheating HLLCHC flux, AR_scheme 22)
+@pytest.mark.parametrize("precision,scheme", [("mixed", 2), ("fp64", 2), ("fp64", 22)])
+def test_result_same_alone_and_in_the_mix(gpu, precision, scheme):
     from overheatingproblem_b200.server import Server
     prec = gpu.lib.MIXED if precision == "mixed" else gpu.lib.FP64
     reqs = mix(gpu)
-    with Server(precision=prec, scheme=2) as srv:
+    with Server(precision=prec, scheme=scheme) as srv:
         mixed = srv.run_trace(reqs, np.zeros(len(reqs)), keep_results=True)["results"]
     for i, req in enumerate(reqs):
-        with Server(precision=prec, scheme=2) as srv:
+        with Server(precision=prec, scheme=scheme) as srv:
             alone = srv.run_trace([req], [0.0], keep_results=True)["results"][0]
-        ctx = run_alone_ctx(gpu, req, prec)
+        ctx = run_alone_ctx(gpu, req, prec, scheme)
         g = 4
         a, b, c = (x[:, g:-g, g:-g] for x in (alone, mixed[i], ctx))
         assert np.all(np.isfinite(c)), i
