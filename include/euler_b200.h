@@ -250,7 +250,7 @@ typedef struct {
 } eb2_request;
 
 /* scheme as AR_scheme (1/2/3/11/22/33, anything else LLF); recon must be 5;
- * the mixed form needs characteristic and takes 1/2/3/LLF only. */
+ * the mixed form needs characteristic. */
 int eb2_server_create(eb2_server **out, int device, int max_slots,
                       unsigned long long hbm_budget_bytes, int precision, int recon,
                       int characteristic, int weno_z, int scheme, double gamma);

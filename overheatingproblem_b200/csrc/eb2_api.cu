@@ -125,10 +125,8 @@ void set_spacing(eb2_ctx* c, double dx, double dy) {
 // The mixed form implements characteristic WENO5 with the four classical
 // fluxes only.
 int check_precision_flux(const eb2_ctx* c, int flux) {
+    (void)flux;
     if (c->precision != EB2_MIXED) return EB2_OK;
-    if (flux >= FLUX_HLLHC)
-        return fail(EB2_EUNSUPPORTED,
-                    "the mixed form has no heat-conduction fluxes (AR_scheme 11/22/33)");
     if (c->num.recon != 5 || !c->num.characteristic)
         return fail(EB2_EUNSUPPORTED,
                     "the mixed form reconstructs with characteristic WENO5 only");

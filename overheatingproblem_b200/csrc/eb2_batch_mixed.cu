@@ -44,6 +44,9 @@ static cudaError_t by_flux(const BatchLaunch& b, int flux, int stage, cudaStream
         case FLUX_HLL: return one<WZ, FLUX_HLL>(b, stage, s);
         case FLUX_HLLC: return one<WZ, FLUX_HLLC>(b, stage, s);
         case FLUX_ROE: return one<WZ, FLUX_ROE>(b, stage, s);
+        case FLUX_HLLHC: return one<WZ, FLUX_HLLHC>(b, stage, s);
+        case FLUX_HLLCHC: return one<WZ, FLUX_HLLCHC>(b, stage, s);
+        case FLUX_ROEHC: return one<WZ, FLUX_ROEHC>(b, stage, s);
         default: return one<WZ, FLUX_LLF>(b, stage, s);
     }
 }

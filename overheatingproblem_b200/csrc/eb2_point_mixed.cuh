@@ -414,5 +414,102 @@ EB2_HD void llf(const Prim& L, const Prim& R, float gamma, float* F) {
     for (int k = 0; k < 4; k++) F[k] = 0.5f * (FL[k] + FR[k]) - 0.5f * sp * (UR[k] - UL[k]);
 }
 
+// --- the heat-conduction ("anti-overheating") fluxes, AR_scheme 11/22/33 ---
+// The classical solvers above plus the reference's energy-flux term in the
+// jump of the specific internal energy e = p / (rho (gamma - 1)); the
+// algebra follows the FP64 forms (eb2_point_fp64.cuh, include/scheme.h
+// :1860-2136, :2153-2471, :2793-3109) in this file's FP32 style.
+EB2_HD float spec_e(const Prim& s, float igm1) { return s.p * s.ir * igm1; }
+
+// HLLHC: HLL plus (s_L s_R / (s_R - s_L)) (e_R - e_L) rho_HLL on the energy
+// flux in the subsonic branch.
+EB2_HD void hllhc(const Prim& L, const Prim& R, float gamma, float* F) {
+    float aL2 = gamma * L.p * L.ir, aR2 = gamma * R.p * R.ir;
+    float sqL = sqr(L.r), sqR = sqr(R.r);
+    float is = rcp(sqL + sqR);
+    float nbar = (sqL * L.un + sqR * R.un) * is;
+    float eta = 0.5f * sqL * sqR * is * is;
+    float du = R.un - L.un;
+    float dd = sqr(fmaf((sqL * aL2 + sqR * aR2), is, eta * du * du));
+    float sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0f) { pflux(L, F); return; }
+    if (sr <= 0.0f) { pflux(R, F); return; }
+    float FL[4], FR[4];
+    pflux(L, FL);
+    pflux(R, FR);
+    float UL[4] = {L.r, L.r * L.un, L.r * L.ut, L.E}, UR[4] = {R.r, R.r * R.un, R.r * R.ut, R.E};
+    float id = rcp(sr - sl), slsr = sl * sr;
+#pragma unroll
+    for (int k = 0; k < 4; k++) F[k] = (sr * FL[k] - sl * FR[k] + slsr * (UR[k] - UL[k])) * id;
+    const float igm1 = rcp(gamma - 1.0f);
+    const float rho_hll = (sr * R.r - sl * L.r + FL[0] - FR[0]) * id;
+    F[3] = fmaf(slsr * id * (spec_e(R, igm1) - spec_e(L, igm1)), rho_hll, F[3]);
+}
+
+// HLLCHC: HLLC plus (s_L s_R / (s_R - s_L)) (e_R - e_L) times the star
+// density on the energy flux of the star states.
+EB2_HD void hllchc(const Prim& L, const Prim& R, float gamma, float* F) {
+    float aL2 = gamma * L.p * L.ir, aR2 = gamma * R.p * R.ir;
+    float sqL = sqr(L.r), sqR = sqr(R.r);
+    float is = rcp(sqL + sqR);
+    float nbar = (sqL * L.un + sqR * R.un) * is;
+    float eta = 0.5f * sqL * sqR * is * is;
+    float du = R.un - L.un;
+    float dd = sqr(fmaf((sqL * aL2 + sqR * aR2), is, eta * du * du));
+    float sl = nbar - dd, sr = nbar + dd;
+    if (sl >= 0.0f) { pflux(L, F); return; }
+    if (sr <= 0.0f) { pflux(R, F); return; }
+    float mL = L.r * (sl - L.un), mR = R.r * (sr - R.un);
+    float ss = (R.p - L.p + L.un * mL - R.un * mR) * rcp(mL - mR);
+    const Prim& S = ss >= 0.0f ? L : R;
+    float sk = ss >= 0.0f ? sl : sr;
+    float mk = ss >= 0.0f ? mL : mR;
+    float Fk[4];
+    pflux(S, Fk);
+    float f = mk * rcp(sk - ss);                      // star density
+    float e = S.E * S.ir + (ss - S.un) * (ss + S.p * rcp(mk));
+    const float igm1 = rcp(gamma - 1.0f);
+    const float corr = sl * sr * rcp(sr - sl) * (spec_e(R, igm1) - spec_e(L, igm1));
+    F[0] = fmaf(sk, f - S.r, Fk[0]);
+    F[1] = fmaf(sk, fmaf(f, ss, -S.r * S.un), Fk[1]);
+    F[2] = fmaf(sk, fmaf(f, S.ut, -S.r * S.ut), Fk[2]);
+    F[3] = fmaf(corr, f, fmaf(sk, fmaf(f, e, -S.E), Fk[3]));
+}
+
+// RoeHC: Roe with 1e-12 in the 1/(2 c^2) and 1/c^2 wave-strength factors,
+// minus 1/2 |u_n + c| (e_R - e_L) rho_bar on the energy flux.
+EB2_HD void roehc(const Prim& L, const Prim& R, float gamma, float* F) {
+    float gm1 = gamma - 1.0f;
+    float sqL = sqr(L.r), sqR = sqr(R.r);
+    float is = rcp(sqL + sqR);
+    float wa = sqL * is, wb = sqR * is;
+    float un = wa * L.un + wb * R.un, ut = wa * L.ut + wb * R.ut;
+    float dun = R.un - L.un, dut = R.ut - L.ut;
+    float hL = gamma / gm1 * L.p * L.ir, hR = gamma / gm1 * R.p * R.ir;
+    float c2 = gm1 * (wa * hL + wb * hR + 0.5f * wa * wb * (dun * dun + dut * dut));
+    float c = sqr(c2);
+    float q2 = un * un + ut * ut;
+    float H = c2 / gm1 + 0.5f * q2;
+    float rbar = sqL * sqR;
+    float dp = R.p - L.p, drho = R.r - L.r;
+    float i2c2 = rcp(fmaf(2.0f, c2, 1.0e-12f)), ic2 = rcp(c2 + 1.0e-12f);
+    float a0 = (dp - rbar * c * dun) * i2c2;
+    float a1 = drho - dp * ic2;
+    float a2 = rbar * dut;
+    float a3 = (dp + rbar * c * dun) * i2c2;
+    float l0 = 0.5f * fabsf(un - c) * a0, l1 = 0.5f * fabsf(un) * a1;
+    float l2 = 0.5f * fabsf(un) * a2, l3 = 0.5f * fabsf(un + c) * a3;
+    float FL[4], FR[4];
+    pflux(L, FL);
+    pflux(R, FR);
+    const float igm1 = rcp(gm1);
+    F[0] = 0.5f * (FL[0] + FR[0]) - (l0 + l1 + l3);
+    F[1] = 0.5f * (FL[1] + FR[1]) - (l0 * (un - c) + l1 * un + l3 * (un + c));
+    F[2] = 0.5f * (FL[2] + FR[2]) - (l0 * ut + l1 * ut + l2 + l3 * ut);
+    F[3] = 0.5f * (FL[3] + FR[3]) -
+           (l0 * (H - un * c) + l1 * 0.5f * q2 + l2 * ut + l3 * (H + un * c)) -
+           0.5f * fabsf(un + c) * (spec_e(R, igm1) - spec_e(L, igm1)) * rbar;
+}
+
 }  // namespace f32
 }  // namespace eb2

@@ -276,9 +276,6 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
     if (recon != 5) return fail(EB2_EUNSUPPORTED, "the server runs WENO5 reconstructions");
     if (precision == EB2_MIXED && !characteristic)
         return fail(EB2_EUNSUPPORTED, "the mixed form reconstructs in characteristic variables");
-    if (precision == EB2_MIXED && (scheme == 11 || scheme == 22 || scheme == 33))
-        return fail(EB2_EUNSUPPORTED,
-                    "the mixed form runs the classical fluxes only (not AR_scheme 11/22/33)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(EB2_ECUDA, "no CUDA device available; there is no CPU path");

@@ -12,6 +12,9 @@ static cudaError_t by_flux(const StageArgs& a, cudaStream_t s) {
         case FLUX_HLLC: return mixstage::launch_one<WZ, FLUX_HLLC>(a, s);
         case FLUX_ROE: return mixstage::launch_one<WZ, FLUX_ROE>(a, s);
         case FLUX_LLF: return mixstage::launch_one<WZ, FLUX_LLF>(a, s);
+        case FLUX_HLLHC: return mixstage::launch_one<WZ, FLUX_HLLHC>(a, s);
+        case FLUX_HLLCHC: return mixstage::launch_one<WZ, FLUX_HLLCHC>(a, s);
+        case FLUX_ROEHC: return mixstage::launch_one<WZ, FLUX_ROEHC>(a, s);
         default: return cudaErrorNotSupported;  // no mixed heat-conduction fluxes
     }
 }

@@ -98,6 +98,9 @@ EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
     if (FLUX == FLUX_HLLC) f32::hllc(L, R, gamma, F);
     else if (FLUX == FLUX_ROE) f32::roe(L, R, gamma, F);
     else if (FLUX == FLUX_HLL) f32::hll(L, R, gamma, F);
+    else if (FLUX == FLUX_HLLHC) f32::hllhc(L, R, gamma, F);
+    else if (FLUX == FLUX_HLLCHC) f32::hllchc(L, R, gamma, F);
+    else if (FLUX == FLUX_ROEHC) f32::roehc(L, R, gamma, F);
     else f32::llf(L, R, gamma, F);
     // (mass, normal, tangential, energy) -> (rho, rho u, rho v, rho E)
     out[0] = F[0];

@@ -48,6 +48,9 @@ unsigned fp64_by_flux(int flux, const double* c, double d, const Gas& g, int pos
         case FLUX_HLL: return fp64_face<DIR, RECON, CH, WZ, FLUX_HLL>(c, d, g, pos, F);
         case FLUX_HLLC: return fp64_face<DIR, RECON, CH, WZ, FLUX_HLLC>(c, d, g, pos, F);
         case FLUX_ROE: return fp64_face<DIR, RECON, CH, WZ, FLUX_ROE>(c, d, g, pos, F);
+        case FLUX_HLLHC: return fp64_face<DIR, RECON, CH, WZ, FLUX_HLLHC>(c, d, g, pos, F);
+        case FLUX_HLLCHC: return fp64_face<DIR, RECON, CH, WZ, FLUX_HLLCHC>(c, d, g, pos, F);
+        case FLUX_ROEHC: return fp64_face<DIR, RECON, CH, WZ, FLUX_ROEHC>(c, d, g, pos, F);
         default: return fp64_face<DIR, RECON, CH, WZ, FLUX_LLF>(c, d, g, pos, F);
     }
 }
@@ -58,6 +61,9 @@ unsigned mixed_by_flux(int flux, const double* c, double pthr, const Gas& g, int
         case FLUX_HLL: return mixed_face<DIR, WZ, FLUX_HLL>(c, pthr, g, pos, F);
         case FLUX_HLLC: return mixed_face<DIR, WZ, FLUX_HLLC>(c, pthr, g, pos, F);
         case FLUX_ROE: return mixed_face<DIR, WZ, FLUX_ROE>(c, pthr, g, pos, F);
+        case FLUX_HLLHC: return mixed_face<DIR, WZ, FLUX_HLLHC>(c, pthr, g, pos, F);
+        case FLUX_HLLCHC: return mixed_face<DIR, WZ, FLUX_HLLCHC>(c, pthr, g, pos, F);
+        case FLUX_ROEHC: return mixed_face<DIR, WZ, FLUX_ROEHC>(c, pthr, g, pos, F);
         default: return mixed_face<DIR, WZ, FLUX_LLF>(c, pthr, g, pos, F);
     }
 }

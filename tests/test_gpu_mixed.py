@@ -24,7 +24,9 @@ def pair(gpu, nx, ny, case, **kw):
     return a, b
 
 
-@pytest.mark.parametrize("scheme,wz", [(2, False), (3, False), (2, True), (1, False)])
+# (11/22/33: the heat-conduction fluxes HLLHC, HLLCHC, RoeHC)
+@pytest.mark.parametrize("scheme,wz", [(2, False), (3, False), (2, True), (1, False),
+                                       (11, False), (22, False), (33, False)])
 def test_mixed_four_quadrant_error(gpu, scheme, wz):
     """256^2 four-quadrant problem to t = 0.05: mixed vs FP64 density L1."""
     a, b = pair(gpu, 256, 256, gpu.lib.CASE_FOUR_QUADRANT, recon=5, characteristic=True,
@@ -87,6 +89,23 @@ def test_mixed_wall_heating_profile(gpu):
     prof, ref = rb.mean(axis=1), ra.mean(axis=1)
     k = int(np.argmin(ref[:10]))
     assert int(np.argmin(prof[:10])) == k and prof[k] < 0.97 * np.median(prof[10:40])
+
+
+def test_mixed_wall_heating_with_hllchc(gpu):
+    """The same run with the anti-overheating HLLCHC flux (AR_scheme 22): the
+    mixed form follows FP64 and, like it, has no dip next to the wall."""
+    a, b = pair(gpu, 400, 8, gpu.lib.CASE_WALL_HEATING, recon=5, characteristic=True,
+                weno_z=False)
+    with a, b:
+        a.run(3, 22, 1 / 400, 0.02 / 8, 0.6)
+        b.run(3, 22, 1 / 400, 0.02 / 8, 0.6)
+        assert b.status() == 0
+        ra, rb = interior(a.download())[0], interior(b.download())[0]
+    l1 = float(np.mean(np.abs(ra - rb)))
+    print(f"wall heating HLLCHC mixed vs FP64: L1 {l1:.3e}  Linf {np.max(np.abs(ra - rb)):.3e}")
+    assert l1 < L1_TOL
+    prof = rb.mean(axis=1)
+    assert prof[:4].min() > 0.995 * np.median(prof[10:40])
 
 
 def test_mixed_near_vacuum_path(gpu):

@@ -277,11 +277,3 @@ def test_heat_conduction_flux_removes_the_wall_dip(gpu):
     assert rho2[:4].min() < 0.95 * plateau          # the dip of the plain scheme
     assert rho22[:4].min() > 0.995 * plateau        # gone with the heat-conduction flux
     assert T22[:4].max() < T2[:4].max()
-
-
-def test_mixed_form_rejects_heat_conduction_fluxes(gpu):
-    with make(gpu, 32, 24, precision=gpu.lib.MIXED, recon=5, characteristic=True) as s:
-        s.init_case(gpu.lib.CASE_FOUR_QUADRANT)
-        with pytest.raises(gpu.EB2Error) as ei:
-            s.rk_step(3, 22, 1e-4, 1 / 32, 1 / 24)
-        assert "heat-conduction" in str(ei.value)

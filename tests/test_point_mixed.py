@@ -67,7 +67,7 @@ def smooth_stencil(rng):
     return np.stack([cons(*t) for t in zip(rho, u, v, p)])
 
 
-@pytest.mark.parametrize("flux", [1, 2, 3, 0])
+@pytest.mark.parametrize("flux", [1, 2, 3, 0, 4, 5, 6])
 @pytest.mark.parametrize("direction", [1, 2])
 def test_smooth_faces_agree(pc, flux, direction):
     rng = np.random.default_rng(10 * flux + direction)
@@ -79,7 +79,7 @@ def test_smooth_faces_agree(pc, flux, direction):
     assert worst < 2e-6, worst
 
 
-@pytest.mark.parametrize("flux", [1, 2, 3, 0])
+@pytest.mark.parametrize("flux", [1, 2, 3, 0, 4, 5, 6])
 @pytest.mark.parametrize("wz", [False, True])
 def test_discontinuous_faces_agree(pc, flux, wz):
     """Quadrant states of the four-quadrant problem and a strong shock tube."""
