@@ -103,6 +103,12 @@ int rpf_flux_reconstruction(int scheme, int rows, int cols, double *U, double *f
 int rpf_space_discrete(int rows, int cols, double dx, double dy, const double *f,
                        const double *gf, const double *s, double *lout, const rpf_globals *g);
 
+/* RK1_TimeAd_BS (include/time_advance.h:886): one forward-Euler step of the
+ * backward-step flow on its two blocks, the channel above the step and the
+ * inlet section beside it, with BC_BackwardStep_2D's boundaries. */
+int rpf_rk1_bs(int scheme, int rows, int cols, double *U, double dt, double dx, double dy,
+               const rpf_globals *g);
+
 /* Message of the last failure (thread-local). */
 const char *rpf_last_error(void);
 

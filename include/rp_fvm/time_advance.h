@@ -39,4 +39,14 @@ static inline void RK3_TimeAd(int AR_scheme, int var_, int rows, int cols, int G
     rpf_rk_call(3, AR_scheme, rows, cols, &y[0][0][0], dt, dx, dy, "RK3_TimeAd");
 }
 
+/* RK1_TimeAd_BS (include/time_advance.h:886-1025): the backward-step flow on
+ * two blocks (the channel above the step, the inlet section beside it). */
+static inline void RK1_TimeAd_BS(int AR_scheme, int var_, int rows, int cols, int GC,
+                                 double (*y)[rows][cols], double dt, double dx, double dy) {
+    (void)var_;
+    (void)GC;
+    rpf_globals g = rpf_collect();
+    rpf_check(rpf_rk1_bs(AR_scheme, rows, cols, &y[0][0][0], dt, dx, dy, &g), "RK1_TimeAd_BS");
+}
+
 #endif

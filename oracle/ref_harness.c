@@ -231,3 +231,8 @@ long ref_run(int order, int scheme, int rows, int cols, double *U, double dx, do
 
 int ref_num_threads(void) { return omp_get_max_threads(); }
 void ref_set_threads(int n) { omp_set_num_threads(n); }
+
+/* RK1_TimeAd_BS, include/time_advance.h:886: the two-block backward-step step */
+void ref_rk1_bs(int scheme, int rows, int cols, double *U, double dt, double dx, double dy) {
+    RK1_TimeAd_BS(scheme, var, rows, cols, GhostCell, (double (*)[rows][cols])U, dt, dx, dy);
+}

@@ -129,6 +129,31 @@ def main() -> None:
          lx=lx.value, ly=ly.value, bc=np.array(list(b)))
     manifest["rayleigh_taylor_16x64_t0.5"] = f"{n} steps to t={tf.value}, gravity source"
 
+    # 2c. backward step (TestCase2D 20) by the reference's two-block
+    #     RK1_TimeAd_BS (include/time_advance.h:886): 40 x 20 from the case's
+    #     Init_Euler_2D state, HLLC, dt = 0.1 dx (the caller's step control),
+    #     6 steps; component WENO5 without source, and characteristic WENO5 with
+    #     the gravity source
+    ref.lib.ref_rk1_bs.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_double,
+                                   C.c_double, C.c_double]
+    for tag, ch, src in (("comp", 0, 0), ("char_gravity", 1, 1)):
+        nx, ny = 40, 20
+        rows, cols = nx + 2 * GC, ny + 2 * GC
+        pri = np.zeros((4, rows, cols)); U = np.zeros_like(pri)
+        F = np.zeros_like(pri); G = np.zeros_like(pri)
+        lx, ly, tm = C.c_double(), C.c_double(), C.c_double()
+        ref.lib.ref_set_params(1.4, 0.5, 5, ch, src, 1.0)
+        ref.lib.ref_init(20, rows, cols, _ptr(pri), _ptr(U), _ptr(F), _ptr(G), C.byref(lx),
+                         C.byref(ly), C.byref(tm))
+        U0 = U.copy()
+        dx, dy = lx.value / nx, ly.value / ny
+        dt = 0.1 * dx
+        for _ in range(6):
+            ref.lib.ref_rk1_bs(2, rows, cols, _ptr(U), dt, dx, dy)
+        save(f"backward_step_{tag}_40x20_rk1bs", U0=U0, U=U, dt=dt, dx=dx, dy=dy,
+             characteristic=ch, source=src)
+        manifest[f"backward_step_{tag}_40x20_rk1bs"] = "RK1_TimeAd_BS, 6 steps"
+
     # 3. double Mach reflection with the exact boundary, 48 x 12: one step of
     #    characteristic WENO5-JS + HLLC, which goes non-finite in the reference
     #    (negative interface pressure at the wall next to the shock foot).  HLL

@@ -26,7 +26,8 @@ ENTRY_POINTS = [
     ("scheme.h", "HLLC_Flux"), ("scheme.h", "Roe_Flux"), ("scheme.h", "LLF_Flux"),
     ("scheme.h", "Space_Discrete_Item"), ("CFD_convection.h", "Flux_Reconstruction_RP"),
     ("time_advance.h", "RK1_TimeAd"), ("time_advance.h", "RK2_TimeAd"),
-    ("time_advance.h", "RK3_TimeAd"), ("Error.h", "TEST_Scheme_Error_L1"),
+    ("time_advance.h", "RK3_TimeAd"), ("time_advance.h", "RK1_TimeAd_BS"),
+    ("Error.h", "TEST_Scheme_Error_L1"),
     ("Error.h", "calculate_orders"), ("Error.h", "print_error_table"),
 ]
 

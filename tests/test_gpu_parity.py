@@ -5,6 +5,7 @@ no stencil reads them and the reference's outflow fills them in an
 order-dependent way."""
 from __future__ import annotations
 
+import ctypes as C
 import json
 import os
 
@@ -277,3 +278,36 @@ def test_heat_conduction_flux_removes_the_wall_dip(gpu):
     assert rho2[:4].min() < 0.95 * plateau          # the dip of the plain scheme
     assert rho22[:4].min() > 0.995 * plateau        # gone with the heat-conduction flux
     assert T22[:4].max() < T2[:4].max()
+
+
+class _RpfGlobals(C.Structure):
+    """rpf_globals of include/rp_fvm/rpf_runtime.h."""
+    _fields_ = [("gamma", C.c_double), ("cfl", C.c_double), ("gravity", C.c_double),
+                ("time", C.c_double), ("source", C.c_int), ("recon", C.c_int),
+                ("characteristic", C.c_int), ("bc", C.c_int * 4), ("reserved", C.c_int),
+                ("inflow", C.c_double * 4), ("fixed", C.c_double * 16)]
+
+
+@pytest.mark.parametrize("tag,ch,src", [("comp", 0, 0), ("char_gravity", 1, 1)])
+def test_backward_step_two_blocks(gpu, tag, ch, src):
+    """RK1_TimeAd_BS (the reference's two-block backward-step step) through the
+    drop-in runtime: six steps from the case's initial state give the
+    reference's bits, without and with the gravity source."""
+    z = golden(f"backward_step_{tag}_40x20_rk1bs")
+    lib = gpu.lib.library()
+    fn = lib.rpf_rk1_bs
+    fn.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
+                   C.c_double, C.POINTER(_RpfGlobals)]
+    fn.restype = C.c_int
+    lib.rpf_last_error.restype = C.c_char_p
+    g = _RpfGlobals(gamma=1.4, cfl=0.5, gravity=1.0, source=src, recon=5, characteristic=ch)
+    U = np.ascontiguousarray(z["U0"].copy())
+    rows, cols = U.shape[1:]
+    try:
+        for _ in range(6):
+            rc = fn(2, rows, cols, U.ctypes.data_as(C.POINTER(C.c_double)), float(z["dt"]),
+                    float(z["dx"]), float(z["dy"]), C.byref(g))
+            assert rc == 0, lib.rpf_last_error()
+    finally:
+        lib.rpf_release_all()
+    assert same_bits(U, z["U"]), bit_report(U, z["U"])
