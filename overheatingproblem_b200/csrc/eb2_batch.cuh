@@ -56,6 +56,9 @@ struct BatchLaunch {
     const int2* work;        // device work list: (slot, tile)
     const int* nwork;        // device: number of work items
     int grid;                // persistent CTAs of the stage kernels
+    int bc_blocks;           // ghost-fill blocks per slot (sized for the largest slot)
+    int slot_range;          // slots 0 .. slot_range-1 hold every active one (the
+                             // ghost-fill and end-of-step grids cover only those)
 };
 cudaError_t launch_stage_batch_fp64(const BatchLaunch& b, const Numerics& num, int stage,
                                     cudaStream_t s);

@@ -74,7 +74,7 @@ __global__ void k_bc_batch(const SlotDesc* __restrict__ slots, int stage) {
 }
 
 cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s) {
-    dim3 grid(8, b.nslots);
+    dim3 grid(b.bc_blocks > 0 ? b.bc_blocks : 8, b.slot_range > 0 ? b.slot_range : b.nslots);
     k_bc_batch<<<grid, 256, 0, s>>>(b.slots, stage);
     return cudaGetLastError();
 }
@@ -88,7 +88,7 @@ __global__ void k_finalize_batch(const SlotDesc* __restrict__ slots) {
 }
 
 cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s) {
-    k_finalize_batch<<<b.nslots, 256, 0, s>>>(b.slots);
+    k_finalize_batch<<<b.slot_range > 0 ? b.slot_range : b.nslots, 256, 0, s>>>(b.slots);
     return cudaGetLastError();
 }
 

@@ -104,6 +104,8 @@ struct eb2_server {
     int sms = 148;
     std::map<int, cudaGraphExec_t> graphs;   // persistent grid -> graph
     std::map<int, int> tuned;                // shape class -> persistent grid
+    int bc_blocks = 8;                       // ghost-fill blocks per slot
+    int slot_range = 1;                      // slots the per-slot kernels cover
     long long graph_launches = 0;
 };
 
@@ -125,7 +127,7 @@ int get_graph(eb2_server* s, int grid, cudaGraphExec_t* out) {
         *out = it->second;
         return EB2_OK;
     }
-    BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0};
+    BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0, s->bc_blocks, s->slot_range};
     CKS(stage_batch(s, b, 0));  // kernel attributes, outside the capture
     b.grid = grid;
     cudaGraph_t g = nullptr;
@@ -168,6 +170,22 @@ int rebuild(eb2_server* s) {
         CKS(cudaMallocHost(&s->h_work, (size_t)cap * sizeof(int2)));
         s->work_cap = cap;
         destroy_graphs(s);  // graphs hold the old work-list address
+    }
+    // one ghost-fill thread per ghost column element of the largest active slot
+    // (32 (nx + ny) of them), as the single-solve fill launches
+    long long ghosts = 0;
+    int top = 0;
+    for (int q = 0; q < s->nslots; q++)
+        if (s->slots[q].used && !s->slots[q].done) {
+            ghosts = std::max(ghosts, 32LL * (s->h_desc[q].grid.nx + s->h_desc[q].grid.ny));
+            top = q + 1;
+        }
+    const int bc_blocks = (int)std::min<long long>(std::max<long long>((ghosts + 255) / 256, 8), 1024);
+    const int slot_range = std::max(top, 1);
+    if (bc_blocks != s->bc_blocks || slot_range != s->slot_range) {
+        s->bc_blocks = bc_blocks;
+        s->slot_range = slot_range;
+        destroy_graphs(s);  // graphs hold the per-slot grids
     }
     CKS(cudaStreamSynchronize(s->stream));  // the pinned staging arrays are reused
     int w = 0;
