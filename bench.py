@@ -570,7 +570,7 @@ def run_ours(args, world, rank, local):
                           "roofline_frac": n2 * n2 * BYTES_PER_CELL_STEP * k / (stm * 1e-3) / 1e9
                           / peak}
         if rank == 0:
-            extra["served_stream"] = serve_stream(eb2, local, 24, args.serve_rate, 7,
+            extra["served_stream"] = serve_stream(eb2, local, 64, args.serve_rate, 7,
                                                   args.serve_baseline)
 
     cpu = None
