@@ -216,15 +216,18 @@ int launch_steps(eb2_server* s) {
     const int cls = shape_class(s->nwork);
     auto it = s->tuned.find(cls);
     if (it == s->tuned.end()) {
-        // autotune: time each persistent-grid candidate on this batch; the
+        // autotune: time each grid candidate on this batch; the
         // slots advance during the trials, which is ordinary progress
         int best = 0;
         float best_ms = 1e30f;
         cudaEvent_t e0, e1;
         CKS(cudaEventCreate(&e0));
         CKS(cudaEventCreate(&e1));
-        for (int mult = 1; mult <= maxb; mult++) {
-            int grid = std::min(mult * s->sms, std::max(s->nwork, 1));
+        // candidates: persistent grids of 1..maxb CTAs per SM, and one CTA per
+        // tile (the hardware then hands tiles to SMs as they free up)
+        for (int mult = 1; mult <= maxb + 1; mult++) {
+            if (mult == maxb + 1 && s->nwork <= maxb * s->sms) break;
+            int grid = mult <= maxb ? std::min(mult * s->sms, std::max(s->nwork, 1)) : s->nwork;
             cudaGraphExec_t ex;
             if (int r = get_graph(s, grid, &ex)) return r;
             CKS(cudaEventRecord(e0, s->stream));
