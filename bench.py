@@ -68,8 +68,9 @@ def parse():
     ap.add_argument("--serve", type=int, default=None, metavar="N",
                     help="served stream of N requests only (batched vs one-at-a-time)")
     ap.add_argument("--serve-rate", type=float, default=20.0)
-    ap.add_argument("--serve-baseline", type=int, default=24,
-                    help="requests of the stream timed one at a time in FP64")
+    ap.add_argument("--serve-baseline", type=int, default=None,
+                    help="time only the first N requests one at a time in FP64 "
+                         "(default: the whole stream, the same requests as the server)")
     ap.add_argument("--dmr", action="store_true",
                     help="double Mach reflection 1920x480 to t = 0.2, FP64 and mixed")
     ap.add_argument("--accuracy", type=float, default=None, metavar="T",
@@ -124,7 +125,7 @@ def serve_stream(eb2, local, n, rate, seed, baseline_n):
                "non_physical": int((out["status"] != 0).sum())}
     # one-at-a-time plain FP64 launches: each request on its own context,
     # started when it has arrived and the previous one has finished
-    m = min(baseline_n, n)
+    m = n if baseline_n is None else min(baseline_n, n)
     t0 = time.perf_counter()
     fin = np.zeros(m)
     bad = 0

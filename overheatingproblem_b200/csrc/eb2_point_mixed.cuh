@@ -15,11 +15,10 @@
 //    (gamma-1)(dE - dK) with dK the kinetic-energy change written in
 //    differences; cell pressures themselves come from FP64;
 //  * rescaled weights -- the WENO weights are formed with one reciprocal per
-//    side from products of (beta + eps)^2 after scaling the stencil by a power
-//    of two and the (beta + eps) by the power of two of the smallest; eps is
-//    the reference's absolute 1e-15 (Reconstruction.h:1414) carried into the
-//    scaled units.  Where FP32 rounding noise in beta exceeds eps the
-//    candidate values agree to that noise, so the weights it picks do not
+//    side from products of (beta + eps) after scaling them by the power of two
+//    of the smallest; eps is the reference's absolute 1e-15
+//    (Reconstruction.h:1414).  Where FP32 rounding noise in beta exceeds eps
+//    the candidate values agree to that noise, so the weights it picks do not
 //    show in the result.
 // Interfaces next to near-vacuum cells (p < 1e-3 of the mean pressure) get
 // their Roe eigenvectors from FP64 arithmetic.
@@ -198,29 +197,20 @@ EB2_HD void unproject(const Eig& e, const float* w, float* q) {
 template <bool WZ>
 EB2_HD void weno5_pair(float w0, float w1, float w3, float w4, float w5,
                                            float& qm, float& qp) {
-    // scale the stencil by the power of two 2^-e of its largest magnitude
-    // s = m 2^e (exact), so that every value lies in (-2, 2) and the products
-    // of (beta + eps)^2 below stay inside the FP32 range
-    float s = fmaxf(fmaxf(fmaxf(fabsf(w0), fabsf(w1)), fmaxf(fabsf(w3), fabsf(w4))), fabsf(w5));
-    int ex = (bits_of(s) >> 23) & 0xff;
-    if (!(s > 0.0f) || ex == 0xff || ex < 2) {  // flat, non-finite or denormal stencil
-        qm = qp = (s == 0.0f || ex < 2) ? 0.0f : s;
+    // a flat stencil reconstructs its base value on both sides (uniform
+    // regions, where whole warps take this branch)
+    if (fmaxf(fmaxf(fmaxf(fabsf(w0), fabsf(w1)), fmaxf(fabsf(w3), fabsf(w4))), fabsf(w5)) ==
+        0.0f) {
+        qm = qp = 0.0f;
         return;
     }
-    const float sc = float_of((254 - ex) << 23), inv_sc = float_of(ex << 23);
-    w0 *= sc;
-    w1 *= sc;
-    w3 *= sc;
-    w4 *= sc;
-    w5 *= sc;
     const float k13 = 13.0f / 12.0f;
-    // The reference's absolute epsilon (1e-15 on the unscaled smoothness
-    // indicators, Reconstruction.h WENO5-JS/Z) in the scaled units: 1e-15 sc^2,
-    // clamped to the normal FP32 range.  Above the clamp beta / eps is below FP32
-    // resolution (linear weights either way); below it eps only matters for a
-    // beta that is exactly zero.
-    const int e2 = min(max(2 * (127 - ex), -75), 100);
-    const float eps = 1.0e-15f * float_of((127 + e2) << 23);
+    // The reference's absolute epsilon of the smoothness indicators
+    // (Reconstruction.h WENO5-JS/Z).  The weights below depend only on ratios
+    // of (beta + eps), which side() brings into range itself, so the stencil
+    // needs no scaling: FP32 rounding is relative, and a beta that underflows
+    // is far below eps either way.
+    const float eps = 1.0e-15f;
     // second differences shared by both sides
     float a1 = fmaf(-2.0f, w1, w0);          // w0 - 2 w1 + w2
     float a2 = w1 + w3;                      // w1 - 2 w2 + w3
@@ -249,9 +239,14 @@ EB2_HD void weno5_pair(float w0, float w1, float w3, float w4, float w5,
     auto side = [&](float b1, float b2, float b3, float k1, float k2, float k3) {
         float t1 = b1 + eps, t2 = b2 + eps, t3 = b3 + eps;
         // The weights are ratios: divide by the power of two of the smallest t
-        // (which lands in [1, 2)) and cap the others at 2^30, past which their
-        // weight is below FP32 resolution, so no product below leaves the range.
-        const float tm = fminf(fminf(t1, t2), t3);
+        // (which lands in [1, 2); a smallest t above 2^100, or NaN, counts as
+        // 2^100) and cap the others at 2^30, past which their weight is below
+        // 2^-60 of the largest (a flat side next to a jump keeps its value to
+        // that level).  The linear weights carry a factor 2^-64 (JS) or 2^-32
+        // (Z), exact, so every g lies in [2^-68, 2^57] and the candidate values
+        // k (linear in the stencil) can reach 2^70 before the weighted sum
+        // leaves the FP32 range.
+        const float tm = fminf(fminf(fminf(t1, t2), t3), 0x1p100f);
         const float nrm = float_of((254 - (int)((bits_of(tm) >> 23) & 0xff)) << 23);
         t1 = fminf(t1 * nrm, 1073741824.0f);
         t2 = fminf(t2 * nrm, 1073741824.0f);
@@ -261,20 +256,20 @@ EB2_HD void weno5_pair(float w0, float w1, float w3, float w4, float w5,
             // WENO-Z (Reconstruction.h:1546-1551): a_k = d_k (1 + tau5 / (beta_k + eps))
             float tau = fabsf(t1 - t3);
             float p23 = t2 * t3, p13 = t1 * t3, p12 = t1 * t2;
-            g1 = 0.1f * (p23 * t1 + tau * p23);
-            g2 = 0.6f * (p13 * t2 + tau * p13);
-            g3 = 0.3f * (p12 * t3 + tau * p12);
+            g1 = (0.1f * 0x1p-32f) * (p23 * t1 + tau * p23);
+            g2 = (0.6f * 0x1p-32f) * (p13 * t2 + tau * p13);
+            g3 = (0.3f * 0x1p-32f) * (p12 * t3 + tau * p12);
         } else {
             float q1 = t1 * t1, q2 = t2 * t2, q3 = t3 * t3;
-            g1 = 0.1f * (q2 * q3);
-            g2 = 0.6f * (q1 * q3);
-            g3 = 0.3f * (q1 * q2);
+            g1 = (0.1f * 0x1p-64f) * (q2 * q3);
+            g2 = (0.6f * 0x1p-64f) * (q1 * q3);
+            g3 = (0.3f * 0x1p-64f) * (q1 * q2);
         }
         float r = rcp(g1 + g2 + g3) * (1.0f / 6.0f);
         return fmaf(g1, k1, fmaf(g2, k2, g3 * k3)) * r;
     };
-    qm = side(bL1, bL2, bL3, cl1, c2, c3) * inv_sc;
-    qp = side(bR1, bR2, bR3, cr1, cr2, cr3) * inv_sc;
+    qm = side(bL1, bL2, bL3, cl1, c2, c3);
+    qp = side(bR1, bR2, bR3, cr1, cr2, cr3);
 }
 
 // Interface state in primitive form from the base cell and a conserved

@@ -121,3 +121,42 @@ def test_near_vacuum_uses_fp64_eigenvectors(pc):
     a, b, _, _ = faces(pc, cells, 1, 2, pthr=1e-6)
     assert np.all(np.isfinite(b))
     assert np.max(np.abs(a - b) / (np.abs(a) + 1e-6)) < 1e-4
+
+
+@pytest.mark.parametrize("scale", [1e-6, 1e-3, 1e3, 1e8])
+@pytest.mark.parametrize("wz", [False, True])
+def test_scaled_states_agree(pc, scale, wz):
+    """rho and p times a common factor (the fluxes scale with it): the weights
+    depend on the absolute eps of the reference in both forms, and FP32
+    rounding stays relative to the jumps at every magnitude."""
+    base = [(1.0, 0.75, 0.0, 1.0), (0.125, 0.0, 0.3, 0.1), (1.5, -0.5, 0.2, 1.5)]
+    worst, compared = 0.0, 0
+    for sa in base:
+        for sb in base:
+            for cut in range(1, 6):
+                ca = cons(scale * sa[0], sa[1], sa[2], scale * sa[3])
+                cb = cons(scale * sb[0], sb[1], sb[2], scale * sb[3])
+                cells = np.stack([ca] * cut + [cb] * (6 - cut))
+                for d in (1, 2):
+                    a, b, s1, s2 = faces(pc, cells, d, 2, wz)
+                    assert s1 == s2
+                    if s1 == 0:
+                        compared += 1
+                        worst = max(worst, float(np.max(np.abs(a - b) / (np.abs(a) + scale))))
+    assert compared >= 80, compared
+    assert worst < 1e-5, worst
+
+
+@pytest.mark.parametrize("flux", [1, 2, 3, 0, 4, 5, 6])
+def test_uniform_stencils_agree(pc, flux):
+    """Six equal states: every characteristic difference is zero and WENO
+    returns the cell state on both sides without forming weights."""
+    worst = 0.0
+    for st in [cons(1.5, 0, 0, 1.5), cons(0.138, 1.206, 1.206, 0.029), cons(1.0, -1.0, 0, 1e-4),
+               cons(8.0, 7.14, -4.125, 116.5)]:
+        for d in (1, 2):
+            a, b, s1, s2 = faces(pc, np.stack([st] * 6), d, flux)
+            assert s1 == 0 and s2 == 0
+            worst = max(worst, float(np.max(np.abs(a - b) / (np.abs(a) + 1.0))))
+    assert worst < 1e-6, worst
+
