@@ -7,6 +7,8 @@
 // locations are cited per function.
 #pragma once
 
+#include <cstring>
+
 #include "eb2_common.cuh"
 #include "eb2_fdiv.cuh"
 
@@ -332,22 +334,43 @@ EB2_HD double weno3_rn(double v1, double v2, double v3, DivGuard& gd) {
 #endif
 }
 
+// q[n0..n1) all have the bits of q[2] (integer compares, off the FP64 pipe).
+EB2_HD bool same_bits(const double* q, int n0, int n1) {
+#if defined(__CUDA_ARCH__)
+    const unsigned h = __double2hiint(q[2]), l = __double2loint(q[2]);
+    unsigned d = 0u;
+    for (int n = n0; n < n1; n++)
+        d |= (__double2hiint(q[n]) ^ h) | (__double2loint(q[n]) ^ l);
+    return d == 0u;
+#else
+    for (int n = n0; n < n1; n++)
+        if (memcmp(&q[n], &q[2], sizeof(double)) != 0) return false;
+    return true;
+#endif
+}
+
 // recon_pair for RECON 5 and 3 through the routines above; the caller checks
-// gd.ok() and recomputes with recon_pair when it fails.
+// gd.ok() and recomputes with recon_pair when it fails.  Where the stencil
+// values all have the same bits (uniform regions), both sides are the same
+// function of the same operands, weno(v, v, v, v, v) or weno3(v, v, v), so the
+// plus side takes the minus side's bits instead of a second evaluation.
 template <int RECON, bool WZ>
 EB2_HD void recon_pair_rn(const double* q, double& qm, double& qp, DivGuard& gd) {
     static_assert(RECON == 5 || RECON == 3, "WENO only");
     if (RECON == 5) {
         if (WZ) {
             qm = weno5_z_rn(q[0], q[1], q[2], q[3], q[4], gd);
-            qp = weno5_z_rn(q[5], q[4], q[3], q[2], q[1], gd);
+            if (same_bits(q, 0, 6)) qp = qm;
+            else qp = weno5_z_rn(q[5], q[4], q[3], q[2], q[1], gd);
         } else {
             qm = weno5_js_rn(q[0], q[1], q[2], q[3], q[4], gd);
-            qp = weno5_js_rn(q[5], q[4], q[3], q[2], q[1], gd);
+            if (same_bits(q, 0, 6)) qp = qm;
+            else qp = weno5_js_rn(q[5], q[4], q[3], q[2], q[1], gd);
         }
     } else {
         qm = weno3_rn(q[1], q[2], q[3], gd);
-        qp = weno3_rn(q[4], q[3], q[2], gd);
+        if (same_bits(q, 1, 5)) qp = qm;
+        else qp = weno3_rn(q[4], q[3], q[2], gd);
     }
 }
 
