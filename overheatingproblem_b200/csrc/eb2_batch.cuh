@@ -59,6 +59,8 @@ struct BatchLaunch {
     int bc_blocks;           // ghost-fill blocks per slot (sized for the largest slot)
     int slot_range;          // slots 0 .. slot_range-1 hold every active one (the
                              // ghost-fill and end-of-step grids cover only those)
+    int each = 0;            // 1: one CTA per work item (grid >= every work-list
+                             // length it is used with), 0: persistent CTAs that loop
 };
 cudaError_t launch_stage_batch_fp64(const BatchLaunch& b, const Numerics& num, int stage,
                                     cudaStream_t s);

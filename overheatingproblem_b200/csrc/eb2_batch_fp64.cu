@@ -22,10 +22,31 @@ __global__ void __launch_bounds__(fp64stage::NT, 2)
     }
 }
 
+// One CTA per work item, the stage arguments in shared memory (as in the
+// mixed form's k_stage_batch_mixed_each).
+template <int RECON, bool CHAR, bool WZ, int FLUX>
+__global__ void __launch_bounds__(fp64stage::NT, 2)
+    k_stage_batch_each(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
+                       const int* __restrict__ nwork, int stage) {
+    __shared__ StageArgs sa;
+    __shared__ int3 tile;
+    if ((int)blockIdx.x >= *nwork) return;
+    if (threadIdx.x == 0) {
+        const int2 it = work[blockIdx.x];
+        const SlotDesc& sd = slots[it.x];
+        sa = slot_args(sd, stage);
+        const int ti = it.y / sd.tiles_x;
+        tile = make_int3(ti, it.y - ti * sd.tiles_x, sd.tiles_x);
+    }
+    __syncthreads();
+    fp64stage::stage_tile<RECON, CHAR, WZ, FLUX>(sa, tile.x, tile.y, tile.z);
+}
+
 template <int RECON, bool CHAR, bool WZ, int FLUX>
 static cudaError_t one(const BatchLaunch& b, int stage, cudaStream_t s) {
     constexpr size_t bytes = fp64stage::smem_bytes<CHAR>();
     auto kern = k_stage_batch<RECON, CHAR, WZ, FLUX>;
+    auto kern_each = k_stage_batch_each<RECON, CHAR, WZ, FLUX>;
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -33,11 +54,17 @@ static cudaError_t one(const BatchLaunch& b, int stage, cudaStream_t s) {
     if (!configured[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)bytes);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(kern_each, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)bytes);
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
     if (b.grid <= 0) return cudaSuccess;  // configuration only
-    kern<<<b.grid, fp64stage::NT, bytes, s>>>(b.slots, b.work, b.nwork, stage);
+    if (b.each)
+        kern_each<<<b.grid, fp64stage::NT, bytes, s>>>(b.slots, b.work, b.nwork, stage);
+    else
+        kern<<<b.grid, fp64stage::NT, bytes, s>>>(b.slots, b.work, b.nwork, stage);
     return cudaGetLastError();
 }
 

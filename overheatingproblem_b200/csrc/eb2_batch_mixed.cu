@@ -20,9 +20,32 @@ __global__ void __launch_bounds__(mixstage::NT, 4)
     }
 }
 
+// One CTA per work item.  With no loop around the tile body, and the stage
+// arguments in shared memory (read there as the single-solve kernel reads its
+// parameter block), nothing but the tile's own values needs registers: the
+// looping kernel spills 20-50 bytes per thread, this one none.
+template <bool WZ, int FLUX>
+__global__ void __launch_bounds__(mixstage::NT, 4)
+    k_stage_batch_mixed_each(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
+                             const int* __restrict__ nwork, int stage) {
+    __shared__ StageArgs sa;
+    __shared__ int3 tile;
+    if ((int)blockIdx.x >= *nwork) return;
+    if (threadIdx.x == 0) {
+        const int2 it = work[blockIdx.x];
+        const SlotDesc& sd = slots[it.x];
+        sa = slot_args(sd, stage);
+        const int ti = it.y / sd.tiles_x;
+        tile = make_int3(ti, it.y - ti * sd.tiles_x, sd.tiles_x);
+    }
+    __syncthreads();
+    mixstage::stage_tile<WZ, FLUX>(sa, tile.x, tile.y, tile.z);
+}
+
 template <bool WZ, int FLUX>
 static cudaError_t one(const BatchLaunch& b, int stage, cudaStream_t s) {
     auto kern = k_stage_batch_mixed<WZ, FLUX>;
+    auto kern_each = k_stage_batch_mixed_each<WZ, FLUX>;
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -30,11 +53,17 @@ static cudaError_t one(const BatchLaunch& b, int stage, cudaStream_t s) {
     if (!configured[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)mixstage::SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(kern_each, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)mixstage::SMEM);
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
     if (b.grid <= 0) return cudaSuccess;  // configuration only
-    kern<<<b.grid, mixstage::NT, mixstage::SMEM, s>>>(b.slots, b.work, b.nwork, stage);
+    if (b.each)
+        kern_each<<<b.grid, mixstage::NT, mixstage::SMEM, s>>>(b.slots, b.work, b.nwork, stage);
+    else
+        kern<<<b.grid, mixstage::NT, mixstage::SMEM, s>>>(b.slots, b.work, b.nwork, stage);
     return cudaGetLastError();
 }
 

@@ -102,8 +102,8 @@ struct eb2_server {
     bool dirty = true;
     long long next_id = 0;
     int sms = 148;
-    std::map<int, cudaGraphExec_t> graphs;   // persistent grid -> graph
-    std::map<int, int> tuned;                // shape class -> persistent grid
+    std::map<int, cudaGraphExec_t> graphs;   // launch key (grid_key) -> graph
+    std::map<int, int> tuned;                // shape class -> launch key
     int bc_blocks = 8;                       // ghost-fill blocks per slot
     int slot_range = 1;                      // slots the per-slot kernels cover
     long long graph_launches = 0;
@@ -121,15 +121,20 @@ cudaError_t stage_batch(eb2_server* s, const BatchLaunch& b, int stage) {
                                      : launch_stage_batch_fp64(b, s->num, stage, s->stream);
 }
 
-int get_graph(eb2_server* s, int grid, cudaGraphExec_t* out) {
-    auto it = s->graphs.find(grid);
+// A stage-kernel launch shape: `grid` CTAs, looping over the work list
+// (each = 0) or one per work item (each = 1, grid >= the work-list length).
+int grid_key(int grid, int each) { return 2 * grid + each; }
+
+int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
+    auto it = s->graphs.find(key);
     if (it != s->graphs.end()) {
         *out = it->second;
         return EB2_OK;
     }
     BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0, s->bc_blocks, s->slot_range};
     CKS(stage_batch(s, b, 0));  // kernel attributes, outside the capture
-    b.grid = grid;
+    b.grid = key / 2;
+    b.each = key % 2;
     cudaGraph_t g = nullptr;
     CKS(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
@@ -149,7 +154,7 @@ int get_graph(eb2_server* s, int grid, cudaGraphExec_t* out) {
     e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     if (e) return fail(EB2_ECUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
-    s->graphs[grid] = ex;
+    s->graphs[key] = ex;
     *out = ex;
     return EB2_OK;
 }
@@ -210,7 +215,7 @@ int shape_class(int nwork) {
     return c;
 }
 
-// One graph launch (kStepsPerGraph batch steps) with the tuned persistent grid.
+// One graph launch (kStepsPerGraph batch steps) with the tuned launch shape.
 int launch_steps(eb2_server* s) {
     const int maxb = stage_batch_max_blocks_per_sm(s->precision == EB2_MIXED ? 1 : 0);
     const int cls = shape_class(s->nwork);
@@ -223,13 +228,17 @@ int launch_steps(eb2_server* s) {
         cudaEvent_t e0, e1;
         CKS(cudaEventCreate(&e0));
         CKS(cudaEventCreate(&e1));
-        // candidates: persistent grids of 1..maxb CTAs per SM, and one CTA per
-        // tile (the hardware then hands tiles to SMs as they free up)
-        for (int mult = 1; mult <= maxb + 1; mult++) {
-            if (mult == maxb + 1 && s->nwork <= maxb * s->sms) break;
-            int grid = mult <= maxb ? std::min(mult * s->sms, std::max(s->nwork, 1)) : s->nwork;
+        // candidates: persistent grids of 1..maxb CTAs per SM smaller than the
+        // work list, and one CTA per work item (the hardware then hands tiles to
+        // SMs as they free up) over 2^cls CTAs, which covers every work-list
+        // length of this shape class
+        std::vector<int> keys;
+        for (int mult = 1; mult <= maxb; mult++)
+            if (mult * s->sms < s->nwork) keys.push_back(grid_key(mult * s->sms, 0));
+        keys.push_back(grid_key(1 << cls, 1));
+        for (int key : keys) {
             cudaGraphExec_t ex;
-            if (int r = get_graph(s, grid, &ex)) return r;
+            if (int r = get_graph(s, key, &ex)) return r;
             CKS(cudaEventRecord(e0, s->stream));
             CKS(cudaGraphLaunch(ex, s->stream));
             CKS(cudaEventRecord(e1, s->stream));
@@ -239,7 +248,7 @@ int launch_steps(eb2_server* s) {
             s->graph_launches++;
             if (ms < best_ms) {
                 best_ms = ms;
-                best = grid;
+                best = key;
             }
         }
         cudaEventDestroy(e0);
