@@ -107,22 +107,30 @@ def stream_trace(n, rate, seed, eb2):
     return reqs, arrivals
 
 
-def serve_stream(eb2, local, n, rate, seed, baseline_n):
+def serve_stream(eb2, local, n, rate, seed, baseline_n, reps=3):
     """Batched mixed-precision server vs one-at-a-time plain FP64 solves on the
-    same trace: solves/s and latency percentiles (finish - arrival)."""
+    same trace: solves/s and latency percentiles (finish - arrival); the server
+    side is the median of `reps` replays."""
     import numpy as np
 
     from overheatingproblem_b200.server import Server
     reqs, arr = stream_trace(n, rate, seed, eb2)
+    # The trace is replayed in real time, so how requests meet in batches (and the
+    # rate) varies from replay to replay: three replays, the median one reported.
+    runs = []
     with Server(device=local, precision=eb2.lib.MIXED, scheme=2,
                 hbm_budget=120 * 10**9) as srv:
-        out = srv.run_trace(reqs, arr)
+        for _ in range(reps):
+            runs.append(srv.run_trace(reqs, arr))
+    runs.sort(key=lambda o: o["makespan"])
+    out = runs[len(runs) // 2]
     lat = out["finish"] - arr
     batched = {"solves_per_s": n / out["makespan"], "makespan_s": out["makespan"],
                "p50_latency_s": float(np.percentile(lat, 50)),
                "p99_latency_s": float(np.percentile(lat, 99)), "requests": n,
                "steps": int(out["steps"].sum()),
-               "non_physical": int((out["status"] != 0).sum())}
+               "non_physical": int((out["status"] != 0).sum()),
+               "replays_solves_per_s": [n / o["makespan"] for o in runs]}
     # one-at-a-time plain FP64 launches: each request on its own context,
     # started when it has arrived and the previous one has finished
     m = n if baseline_n is None else min(baseline_n, n)
