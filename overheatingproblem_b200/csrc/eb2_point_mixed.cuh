@@ -14,10 +14,8 @@
 //    H - q^2/2, b2 = b1 q^2 / 2, and interface pressures are p_base +
 //    (gamma-1)(dE - dK) with dK the kinetic-energy change written in
 //    differences; cell pressures themselves come from FP64;
-//  * weights in range -- the JS weights d / (beta + eps)^2 come from SFU
-//    reciprocals (eps keeps them below 1e30); the WENO-Z weights are formed
-//    with one reciprocal per side from products of (beta + eps) after scaling
-//    them by the power of two of the smallest.  eps is the reference's
+//  * weights in range -- the JS and WENO-Z weights come from SFU reciprocals
+//    of beta + eps (eps keeps them below 1e15).  eps is the reference's
 //    absolute 1e-15 (Reconstruction.h:1414).  Where FP32 rounding noise in beta
 //    exceeds eps the candidate values agree to that noise, so the weights it
 //    picks do not show in the result.
@@ -48,24 +46,6 @@ EB2_HD float rsq(float x) {
     return r;
 #else
     return 1.0f / sqrtf(x);
-#endif
-}
-EB2_HD int bits_of(float x) {
-#ifdef __CUDA_ARCH__
-    return __float_as_int(x);
-#else
-    int i;
-    memcpy(&i, &x, sizeof i);
-    return i;
-#endif
-}
-EB2_HD float float_of(int i) {
-#ifdef __CUDA_ARCH__
-    return __int_as_float(i);
-#else
-    float x;
-    memcpy(&x, &i, sizeof x);
-    return x;
 #endif
 }
 EB2_HD float sqr(float x) { return x * rsq(x); }  // sqrt for x > 0
@@ -239,36 +219,24 @@ EB2_HD void weno5_pair(float w0, float w1, float w3, float w4, float w5,
     float cr3 = fmaf(5.0f, r2, -r1);         // stencil i-1..i+1
     auto side = [&](float b1, float b2, float b3, float k1, float k2, float k3) {
         float t1 = b1 + eps, t2 = b2 + eps, t3 = b3 + eps;
-        if (!WZ) {
-            // JS weights d_k / t_k^2 from SFU reciprocals: t >= eps keeps 1/t^2 below
-            // 1e30, and a t so large that its weight flushes to zero has a
-            // negligible weight anyway; the floor on the sum only keeps a stencil
-            // whose three weights all flush (|values| beyond 1e9) finite
-            const float r1 = rcp(t1), r2 = rcp(t2), r3 = rcp(t3);
-            const float g1 = (0.1f * r1) * r1, g2 = (0.6f * r2) * r2, g3 = (0.3f * r3) * r3;
-            const float r = rcp(fmaxf(g1 + g2 + g3, 0x1p-126f)) * (1.0f / 6.0f);
-            return fmaf(g1, k1, fmaf(g2, k2, g3 * k3)) * r;
+        // Weights from SFU reciprocals of t = beta + eps >= eps (so 1/t < 1e15):
+        // JS d_k / t_k^2 (Reconstruction.h WENO5-JS), WENO-Z d_k (1 + tau5 / t_k)
+        // (Reconstruction.h:1546-1551).  A t so large that its weight flushes to
+        // zero has a negligible weight anyway; the floor on the sum only keeps a
+        // stencil whose three weights all flush (|values| beyond 1e9) finite.
+        const float r1 = rcp(t1), r2 = rcp(t2), r3 = rcp(t3);
+        float g1, g2, g3;
+        if (WZ) {
+            const float tau = fabsf(b1 - b3);
+            g1 = 0.1f * fmaf(tau, r1, 1.0f);
+            g2 = 0.6f * fmaf(tau, r2, 1.0f);
+            g3 = 0.3f * fmaf(tau, r3, 1.0f);
+        } else {
+            g1 = (0.1f * r1) * r1;
+            g2 = (0.6f * r2) * r2;
+            g3 = (0.3f * r3) * r3;
         }
-        // WENO-Z.  The weights are ratios: divide by the power of two of the smallest t
-        // (which lands in [1, 2); a smallest t above 2^100, or NaN, counts as
-        // 2^100) and cap the others at 2^30, past which their weight is below
-        // 2^-60 of the largest (a flat side next to a jump keeps its value to
-        // that level).  The linear weights carry an exact factor 2^-32, so every
-        // g lies in [2^-36, 2^59] and the candidate values k (linear in the
-        // stencil) can reach 2^68 before the weighted sum leaves the FP32 range.
-        const float tm = fminf(fminf(fminf(t1, t2), t3), 0x1p100f);
-        const float nrm = float_of((254 - (int)((bits_of(tm) >> 23) & 0xff)) << 23);
-        t1 = fminf(t1 * nrm, 1073741824.0f);
-        t2 = fminf(t2 * nrm, 1073741824.0f);
-        t3 = fminf(t3 * nrm, 1073741824.0f);
-        // WENO-Z (Reconstruction.h:1546-1551): a_k = d_k (1 + tau5 / (beta_k + eps)),
-        // times t1 t2 t3
-        float tau = fabsf(t1 - t3);
-        float p23 = t2 * t3, p13 = t1 * t3, p12 = t1 * t2;
-        const float g1 = (0.1f * 0x1p-32f) * (p23 * t1 + tau * p23);
-        const float g2 = (0.6f * 0x1p-32f) * (p13 * t2 + tau * p13);
-        const float g3 = (0.3f * 0x1p-32f) * (p12 * t3 + tau * p12);
-        float r = rcp(g1 + g2 + g3) * (1.0f / 6.0f);
+        const float r = rcp(fmaxf(g1 + g2 + g3, 0x1p-126f)) * (1.0f / 6.0f);
         return fmaf(g1, k1, fmaf(g2, k2, g3 * k3)) * r;
     };
     qm = side(bL1, bL2, bL3, cl1, c2, c3);
