@@ -290,9 +290,13 @@ int eb2_server_run_trace(eb2_server *srv, const eb2_request *reqs, const double 
  *
  * Limits: (nx+8)*(ny+8) <= EB2_NOALLOC_MAX_CELLS, else EB2_EARG.  All calls
  * share the one array: calls that overlap on the GPU (other streams, other
- * host threads) race and must not be issued.  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  The call enqueues
+ * host threads) race and must not be issued.  Each call looks up the array's
+ * device address in the calling thread's current context (cudaGetSymbolAddress,
+ * not a stream operation), so callers on a context of their own get that
+ * context's copy; the first call in a context also loads the library's device
+ * code there, so make that first call before any stream capture.  Every
+ * reconstruction (recon 1/2/3/5) and every AR_scheme of eb2_rk_step (HLL, HLLC,
+ * Roe, the heat-conduction fluxes 11/22/33, LLF) is accepted.  The call enqueues
  * on `cuda_stream` (NULL: the legacy default stream) and returns after the
  * step, with EB2_ENONPHYS if a non-physical state was met.  Nothing in the
  * array has to start at zero: each call clears the control block itself, and

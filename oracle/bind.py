@@ -4,10 +4,16 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, never by the product package.
 
 * ``Oracle``    -- oracle/liboracle.so, the C restatement (euler_oracle.c).
-* ``Reference`` -- oracle/_ref/libref.so (the reference as shipped) or
+* ``Reference`` -- oracle/_ref/libref.so (the reference as shipped),
   oracle/_ref/libref_wjs.so (its characteristic WENO5 switched to Jiang-Shu
-  weights), built from the reference's own sources by oracle/Makefile.  It
-  exists only where the reference tree was present at build time.
+  weights) or oracle/_ref/libref_wjs_dmr.so (that, with the reference's own
+  commented-out BC_DoubleMach_2D calls of the RK stages switched on), built
+  from the reference's own sources by oracle/Makefile.  They exist only where
+  the reference tree was present at build time.
+
+``REFERENCE_TREE`` is the one place that names where the reference's sources
+lie (environment variable EB2_REFERENCE_TREE); only build recipes and the
+checks that compile the reference's own caller read it.
 """
 from __future__ import annotations
 
@@ -19,6 +25,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GC = 4
+REFERENCE_TREE = os.environ.get("EB2_REFERENCE_TREE", "/root/reference")
+
+_VARIANTS = {"": "libref.so", "wjs": "libref_wjs.so", "wjs_dmr": "libref_wjs_dmr.so"}
 
 # BC kinds (include/Boundary_Condition.h:21-27)
 OUTFLOW, REFLECT, PERIODIC, INFLOW, FIXED = 0, 1, 2, 3, 4
@@ -176,10 +185,10 @@ class Reference:
     """The reference compiled from its own sources (oracle/_ref)."""
 
     def __init__(self, variant: str = ""):
-        name = "libref_wjs.so" if variant == "wjs" else "libref.so"
-        path = os.path.join(HERE, "_ref", name)
+        path = os.path.join(HERE, "_ref", _VARIANTS[variant])
         if not os.path.exists(path):
             raise FileNotFoundError(path)
+        self.variant = variant
         lib = C.CDLL(path)
         i, d = C.c_int, C.c_double
         sig = {
@@ -204,6 +213,7 @@ class Reference:
             "ref_run": (C.c_long, [i, i, i, i, _dp, d, d, d, i, i, _dp]),
             "ref_num_threads": (i, []),
             "ref_set_threads": (None, [i]),
+            "ref_set_time": (None, [d]),
         }
         for n_, (res, args) in sig.items():
             fn = getattr(lib, n_)
@@ -213,21 +223,39 @@ class Reference:
 
     @staticmethod
     def available(variant: str = "") -> bool:
-        name = "libref_wjs.so" if variant == "wjs" else "libref.so"
-        return os.path.exists(os.path.join(HERE, "_ref", name))
+        return os.path.exists(os.path.join(HERE, "_ref", _VARIANTS[variant]))
 
     def configure(self, p: OrcParams):
         self.lib.ref_set_params(p.gamma, p.cfl, p.recon, p.characteristic, p.source, p.gravity)
         self.lib.ref_set_bc(p.bc[0], p.bc[1], p.bc[2], p.bc[3])
 
     def rk(self, p, order, scheme, U, dt, dx, dy, t=0.0):
+        """One RKn_TimeAd step.  In the wjs_dmr build the reference's own RK
+        stages fill ghosts with BC_DoubleMach_2D at the global Time = t; in the
+        other builds p.dmr selects the composed ref_rk_dmr."""
         self.configure(p)
         rows, cols = U.shape[1], U.shape[2]
-        if p.dmr:
+        if self.variant == "wjs_dmr":
+            self.lib.ref_set_time(t)
+            self.lib.ref_rk(order, scheme, rows, cols, _ptr(U), dt, dx, dy)
+        elif p.dmr:
             self.lib.ref_rk_dmr(order, scheme, rows, cols, _ptr(U), dt, dx, dy, t)
         else:
             self.lib.ref_rk(order, scheme, rows, cols, _ptr(U), dt, dx, dy)
         return U
+
+    def init(self, test_case: int, nx: int, ny: int):
+        """Init_Euler_2D of one of the reference's own TestCase2D values: the
+        conserved state, the domain lengths and final time, and the boundary
+        kinds the case sets."""
+        rows, cols = nx + 2 * GC, ny + 2 * GC
+        arrs = [np.zeros((4, rows, cols)) for _ in range(4)]
+        lx, ly, tmax = C.c_double(), C.c_double(), C.c_double()
+        self.lib.ref_init(test_case, rows, cols, *(_ptr(a) for a in arrs), C.byref(lx),
+                          C.byref(ly), C.byref(tmax))
+        kinds = (C.c_int * 4)()
+        self.lib.ref_get_bc(kinds)
+        return arrs[1], lx.value, ly.value, tmax.value, tuple(kinds)
 
     def dt(self, p, U, dx, dy) -> float:
         self.configure(p)

@@ -12,7 +12,11 @@
  * function named in its comment; the only composed routine is ref_rk_dmr,
  * which runs the RK stages of include/time_advance.h with the exact
  * double-Mach boundary BC_DoubleMach_2D (include/Boundary_Condition.h:480),
- * whose call sites are commented out in the reference.
+ * whose call sites are commented out in the reference.  A third build,
+ * oracle/_ref/libref_wjs_dmr.so, switches those commented-out calls on inside
+ * the reference's own RK1/RK2/RK3_TimeAd (time_advance.h:591-862), so that
+ * ref_rk there is the reference's own double-Mach step; tests check that
+ * ref_rk_dmr gives the same bits.
  */
 #define main rp_fvm_main
 #include "RP_FVM.c"
@@ -175,6 +179,10 @@ void ref_rk_dmr(int order, int scheme, int rows, int cols, double *U, double dt,
     }
     free(Lt); free(U1); free(U2); free(f); free(g); free(s);
 }
+
+/* The reference's global Time (include/Golbal.h:45): the time BC_DoubleMach_2D
+ * reads in the libref_wjs_dmr.so build, whose RK stages call it. */
+void ref_set_time(double t) { Time = t; }
 
 /* Get_Delta_T_2D, include/function.h:144 */
 double ref_dt(int rows, int cols, double *U, double dx, double dy) {

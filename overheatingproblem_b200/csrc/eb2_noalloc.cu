@@ -11,9 +11,14 @@
 // exits.
 //
 // The host-side name g_scratch is only a stand-in for the device array: a
-// kernel handed it would fault or read the wrong memory.  The device address is
-// obtained once per device with cudaGetSymbolAddress while that device is
-// current, and that address is what the kernels receive.
+// kernel handed it would fault or read the wrong memory.  Every call asks
+// cudaGetSymbolAddress for the array's address in the calling thread's current
+// context, with the target device current, and hands that address to the
+// kernels.  A module-scope __device__ array has one copy per CUDA context, so
+// an address remembered from an earlier call could belong to another context
+// (one the caller created with the driver API, or a primary context that
+// cudaDeviceReset has since replaced); the lookup is not a stream operation and
+// costs far less than the step.
 #include <cstdio>
 #include <cstring>
 
@@ -30,9 +35,6 @@ constexpr size_t kScratchBytes =
 
 // The scratch array.  All calls share it and it keeps the last call's contents.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
-
-constexpr int kMaxDevices = 64;
-unsigned char* g_scratch_dev[kMaxDevices] = {};  // device address per device
 
 __global__ void k_noalloc_begin(Ctrl* c, double t, double dt) {
     // the control block must start from zero on every call
@@ -62,12 +64,9 @@ extern "C" int eb2_rk_step_noalloc(double* U, int nx, int ny, const eb2_noalloc_
     const long long rows = nx + 2LL * GC, cols = ny + 2LL * GC;
     if (rows * cols > (long long)EB2_NOALLOC_MAX_CELLS)
         return fail(EB2_EARG, "grid exceeds EB2_NOALLOC_MAX_CELLS (rows*cols incl. ghosts)");
-    if (cfg->recon != 1 && cfg->recon != 2 && cfg->recon != 5)
-        return fail(EB2_EARG, "recon must be 1, 2 or 5");
+    if (cfg->recon != 1 && cfg->recon != 2 && cfg->recon != 3 && cfg->recon != 5)
+        return fail(EB2_EARG, "recon must be 1, 2, 3 or 5");
     if (!(cfg->gamma > 1.0)) return fail(EB2_EARG, "gamma must exceed 1");
-    if (scheme == 11 || scheme == 22 || scheme == 33)
-        return fail(EB2_EUNSUPPORTED,
-                    "this entry point runs the classical fluxes only (not AR_scheme 11/22/33)");
     int kind[4] = {cfg->bc_left, cfg->bc_right, cfg->bc_bottom, cfg->bc_top};
     for (int s = 0; s < 4; s++) {
         if (kind[s] < BC_OUTFLOW || kind[s] > BC_FIXED) return fail(EB2_EARG, "bad bc kind");
@@ -75,18 +74,12 @@ extern "C" int eb2_rk_step_noalloc(double* U, int nx, int ny, const eb2_noalloc_
         if ((kind[s] == BC_PERIODIC || (kind[s] == BC_REFLECT && (s == 0 || s == 3))) && n < GC)
             return fail(EB2_EUNSUPPORTED, "mirrored or periodic side needs 4 interior cells");
     }
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e) return fail(EB2_ECUDA, "cudaGetDevice", e);
-    if (dev < 0 || dev >= kMaxDevices) return fail(EB2_EARG, "device index too large");
-    // one-time set-up on this device: the device address of the scratch array
-    if (!g_scratch_dev[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e) return fail(EB2_ECUDA, "cudaGetSymbolAddress", e);
-        g_scratch_dev[dev] = (unsigned char*)p;
-    }
-    unsigned char* base = g_scratch_dev[dev];
+    // the device address of the scratch array in the current context (the
+    // first call in a context also loads the library's module there)
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+    if (e) return fail(EB2_ECUDA, "cudaGetSymbolAddress", e);
+    unsigned char* base = (unsigned char*)p;
     Ctrl* ctrl = (Ctrl*)base;
     const size_t nstate = (size_t)4 * rows * cols;
     double* u1 = (double*)(base + kCtrlBytes);
@@ -107,7 +100,14 @@ extern "C" int eb2_rk_step_noalloc(double* U, int nx, int ny, const eb2_noalloc_
     num.recon = cfg->recon;
     num.characteristic = cfg->characteristic ? 1 : 0;
     num.weno_z = cfg->weno_z ? 1 : 0;
-    num.flux = scheme == 1 ? FLUX_HLL : scheme == 2 ? FLUX_HLLC : scheme == 3 ? FLUX_ROE : FLUX_LLF;
+    // AR_scheme numbering of Flux_Reconstruction_RP (include/CFD_convection.h:334-362)
+    num.flux = scheme == 1    ? FLUX_HLL
+               : scheme == 2  ? FLUX_HLLC
+               : scheme == 3  ? FLUX_ROE
+               : scheme == 11 ? FLUX_HLLHC
+               : scheme == 22 ? FLUX_HLLCHC
+               : scheme == 33 ? FLUX_ROEHC
+                              : FLUX_LLF;
     num.source = cfg->source ? 1 : 0;
     num.gravity = cfg->gravity;
     Boundary b{};

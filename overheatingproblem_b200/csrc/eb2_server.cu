@@ -414,13 +414,33 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
     tg.ny = r->ny;
     const int ntiles = stage_blocks(tg, s->precision == EB2_MIXED);
     const int npart = std::max(ntiles, 296);
-    CKS(cudaMallocAsync(&sl.u, n, s->stream));
-    CKS(cudaMallocAsync(&sl.u1, n, s->stream));
-    CKS(cudaMallocAsync(&sl.u2, n, s->stream));
-    CKS(cudaMallocAsync(&sl.partials, (size_t)3 * npart * sizeof(double), s->stream));
-    CKS(cudaMemsetAsync(sl.u, 0, n, s->stream));
-    CKS(cudaMemsetAsync(sl.u1, 0, n, s->stream));
-    CKS(cudaMemsetAsync(sl.u2, 0, n, s->stream));
+    // Any failure from here on releases what this call allocated and leaves
+    // the slot unused, so that a failed admission leaks nothing.
+    auto undo = [&](int code) {
+        double** bufs[4] = {&sl.u, &sl.u1, &sl.u2, &sl.partials};
+        for (double** b : bufs)
+            if (*b) {
+                cudaFreeAsync(*b, s->stream);
+                *b = nullptr;
+            }
+        cudaStreamSynchronize(s->stream);
+        memset(&s->h_desc[q], 0, sizeof(SlotDesc));
+        sl = Slot();
+        return code;
+    };
+#define CKU(expr)                                                                        \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return undo(fail(EB2_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_)));       \
+    } while (0)
+    CKU(cudaMallocAsync(&sl.u, n, s->stream));
+    CKU(cudaMallocAsync(&sl.u1, n, s->stream));
+    CKU(cudaMallocAsync(&sl.u2, n, s->stream));
+    CKU(cudaMallocAsync(&sl.partials, (size_t)3 * npart * sizeof(double), s->stream));
+    CKU(cudaMemsetAsync(sl.u, 0, n, s->stream));
+    CKU(cudaMemsetAsync(sl.u1, 0, n, s->stream));
+    CKU(cudaMemsetAsync(sl.u2, 0, n, s->stream));
     SlotDesc& sd = s->h_desc[q];
     memset(&sd, 0, sizeof sd);
     sd.u = sl.u;
@@ -447,15 +467,17 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
     sd.tiles_x = (r->ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y;
     sd.ntiles = ntiles;
     sd.ncells = r->nx * r->ny;
-    CKS(launch_init(sl.u, sd.grid, sd.gas, d, s->stream));
+    CKU(launch_init(sl.u, sd.grid, sd.gas, d, s->stream));
     // control block and first CFL step, as eb2_run starts a solve
     const double cfl = r->cfl > 0.0 ? r->cfl : 0.5;
     const double dmin = sd.grid.dx > sd.grid.dy ? sd.grid.dy : sd.grid.dx;
-    CKS(cudaMemsetAsync(s->d_ctrl + q, 0, sizeof(Ctrl), s->stream));
+    CKU(cudaMemsetAsync(s->d_ctrl + q, 0, sizeof(Ctrl), s->stream));
     set_loop_ctrl(s->d_ctrl + q, 0.0, T, T, cfl, dmin, LLONG_MAX, s->stream);
+    CKU(cudaGetLastError());
     int nb = 0;
-    CKS(launch_wave_partials(sl.u, sd.grid, sd.gas, sl.partials, &nb, s->stream));
-    CKS(launch_finalize(s->d_ctrl + q, sl.partials, nb, sd.ncells, 1, s->stream));
+    CKU(launch_wave_partials(sl.u, sd.grid, sd.gas, sl.partials, &nb, s->stream));
+    CKU(launch_finalize(s->d_ctrl + q, sl.partials, nb, sd.ncells, 1, s->stream));
+#undef CKU
     sl.used = true;
     sl.done = false;
     sl.id = s->next_id++;

@@ -11,9 +11,10 @@ import subprocess
 import pytest
 
 from conftest import HAVE_GPU, ROOT
+from oracle.bind import REFERENCE_TREE
 
 SHIM = os.path.join(ROOT, "include", "rp_fvm")
-REF_CALLER = "/root/reference/src/RP_FVM.c"
+REF_CALLER = os.path.join(REFERENCE_TREE, "src", "RP_FVM.c")
 
 # (header, entry point) pairs of the reference's operator API the set carries
 ENTRY_POINTS = [

@@ -227,3 +227,41 @@ def test_live_reference_time_loop(oracle):
     assert (na, ta) == (nb, tb)
     m = noncorner_mask(Ua.shape)
     assert same_bits(Ua[:, m], Ub[:, m]), bit_report(Ua[:, m], Ub[:, m])
+
+
+need_dmr = pytest.mark.skipif(not Reference.available("wjs_dmr"),
+                              reason="oracle/_ref not built (needs the reference tree)")
+
+
+@need_dmr
+@pytest.mark.parametrize("scheme", [2, 3])
+def test_double_mach_step_is_the_references_own(oracle, scheme):
+    """One step with the exact double-Mach boundary.  The reference carries a
+    BC_DoubleMach_2D call, commented out, beside each stage's ghost fill of its
+    RK stages (include/time_advance.h:747-862); the wjs_dmr build switches
+    those lines on, so its RK3_TimeAd is the reference's own double-Mach step.
+    The composed ref_rk_dmr, the oracle and the committed golden vector (the
+    GPU's check) all give its bits -- NaNs where the scheme breaks down
+    included.  (HLL is left out: where it skips an interface the reference
+    copies a flux entry it never wrote from an uninitialised temporary, so two
+    reference builds need not agree there.)"""
+    dmr = Reference("wjs_dmr")
+    wjs = Reference("wjs")
+    p = oracle.params(48, 12, recon=5, characteristic=1, weno_z=0, cfl=0.4)
+    U0, lx, ly, _ = oracle.init_case(p, DOUBLE_MACH)
+    p.dmr = 1
+    dx, dy = lx / 48, ly / 12
+    Ua, Ub, Uc = U0.copy(), U0.copy(), U0.copy()
+    for t in (0.0, 1e-3):
+        dt = dmr.dt(p, Ua, dx, dy)
+        assert dt == wjs.dt(p, Ub, dx, dy) == oracle.dt(p, Uc, dx, dy)
+        dmr.rk(p, 3, scheme, Ua, dt, dx, dy, t)
+        wjs.rk(p, 3, scheme, Ub, dt, dx, dy, t)
+        oracle.rk(p, 3, scheme, Uc, dt, dx, dy, t)
+        m = noncorner_mask(Ua.shape)
+        assert same_bits(Ua[:, m], Ub[:, m]), bit_report(Ua[:, m], Ub[:, m])
+        assert same_bits(Ua[:, m], Uc[:, m]), bit_report(Ua[:, m], Uc[:, m])
+        if scheme == 2 and t == 0.0:
+            z = golden("dmr_charjs_hllc_48x12_step1")
+            assert dt == float(z["dt"])
+            assert same_bits(interior(Ua), interior(z["U"]))

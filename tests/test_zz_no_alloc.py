@@ -21,8 +21,22 @@ from conftest import bit_report, noncorner_mask, same_bits
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("order,scheme,recon,ch", [(3, 2, 5, 1), (2, 3, 2, 0)])
-def test_noalloc_step_matches_context_step(gpu, order, scheme, recon, ch):
+# (order, AR_scheme, recon, characteristic, bc kinds left/right/bottom/top,
+# gravity source): the three step orders (order 1 writes into the scratch then
+# copies back), every reconstruction family, a heat-conduction flux, and
+# reflecting, periodic and inflow ghost fills with the gravity source on
+CASES = [
+    (3, 2, 5, 1, (0, 0, 0, 0), 0),
+    (2, 3, 2, 0, (0, 0, 0, 0), 0),
+    (1, 1, 1, 0, (1, 0, 2, 2), 0),
+    (3, 22, 3, 1, (1, 1, 2, 2), 1),
+    (2, 2, 5, 0, (2, 2, 1, 1), 1),
+    (3, 33, 5, 1, (3, 0, 1, 0), 0),
+]
+
+
+@pytest.mark.parametrize("order,scheme,recon,ch,kinds,src", CASES)
+def test_noalloc_step_matches_context_step(gpu, order, scheme, recon, ch, kinds, src):
     import torch
 
     L = gpu.lib
@@ -31,22 +45,30 @@ def test_noalloc_step_matches_context_step(gpu, order, scheme, recon, ch):
     dx, dy = 1.0 / nx, 1.0 / ny
     # the existing entry point: two steps on a context
     ref = []
-    with gpu.Solver(nx, ny, recon=recon, characteristic=bool(ch), weno_z=False) as s:
+    with gpu.Solver(nx, ny, recon=recon, characteristic=bool(ch), weno_z=False,
+                    source=bool(src), gravity=1.0) as s:
         s.init_case(L.CASE_FOUR_QUADRANT)
+        s.set_bc(*kinds)
         U0 = s.download()
         for _ in range(2):
             dt = s.delta_t(dx, dy)
-            s.rk_step(order, scheme, dt, dx, dy)
-            ref.append((dt, s.download()))
-    cfg = L.NoallocConfig(gamma=1.4, recon=recon, characteristic=ch, weno_z=0, bc_left=0,
-                          bc_right=0, bc_bottom=0, bc_top=0, source=0, gravity=1.0)
+            rc = s.rk_step(order, scheme, dt, dx, dy)
+            ref.append((dt, rc, s.download()))
+    cfg = L.NoallocConfig(gamma=1.4, recon=recon, characteristic=ch, weno_z=0,
+                          bc_left=kinds[0], bc_right=kinds[1], bc_bottom=kinds[2],
+                          bc_top=kinds[3], source=src, gravity=1.0)
     # the caller owns the device state; the entry point allocates nothing
     dev = torch.from_numpy(U0).to("cuda")
     stream = torch.cuda.current_stream()
-    for dt, U_ref in ref:
+    seen_nonphys = False
+    for dt, rc_ref, U_ref in ref:
         rc = lib.eb2_rk_step_noalloc(C.c_void_p(dev.data_ptr()), nx, ny, C.byref(cfg), order,
                                      scheme, dt, dx, dy, 0.0, C.c_void_p(stream.cuda_stream))
-        assert rc == L.EB2_OK, lib.eb2_last_error()
+        # the same status as the context step; the context reports a
+        # non-physical state once, the no-allocation step on every call
+        assert rc in (L.EB2_OK, L.EB2_ENONPHYS), lib.eb2_last_error()
+        assert rc == rc_ref or (rc == L.EB2_ENONPHYS and seen_nonphys), lib.eb2_last_error()
+        seen_nonphys = seen_nonphys or rc_ref == L.EB2_ENONPHYS
         got = dev.cpu().numpy()
         m = noncorner_mask(got.shape)
         assert same_bits(got[:, m], U_ref[:, m]), bit_report(got[:, m], U_ref[:, m])
