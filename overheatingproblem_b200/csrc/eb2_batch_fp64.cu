@@ -119,6 +119,5 @@ cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-int stage_batch_max_blocks_per_sm(int precision) { return precision == 0 ? 2 : 4; }
 
 }  // namespace eb2

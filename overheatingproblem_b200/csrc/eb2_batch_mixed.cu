@@ -6,7 +6,7 @@
 namespace eb2 {
 
 template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(mixstage::NT, 4)
+__global__ void __launch_bounds__(mixstage::NT, mixstage::CTAS)
     k_stage_batch_mixed(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
                         const int* __restrict__ nwork, int stage) {
     const int n = *nwork;
@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(mixstage::NT, 4)
 // parameter block), nothing but the tile's own values needs registers: the
 // looping kernel spills 20-50 bytes per thread, this one none.
 template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(mixstage::NT, 4)
+__global__ void __launch_bounds__(mixstage::NT, mixstage::CTAS)
     k_stage_batch_mixed_each(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
                              const int* __restrict__ nwork, int stage) {
     __shared__ StageArgs sa;
@@ -85,5 +85,9 @@ cudaError_t launch_stage_batch_mixed(const BatchLaunch& b, const Numerics& num, 
     if (num.recon != 5 || !num.characteristic) return cudaErrorNotSupported;
     return num.weno_z ? by_flux<true>(b, num.flux, stage, s) : by_flux<false>(b, num.flux, stage, s);
 }
+
+// Resident CTAs per SM of the batched stage kernels: the persistent-grid
+// candidates of the server's autotuner go up to this many per SM.
+int stage_batch_max_blocks_per_sm(int precision) { return precision == 0 ? 2 : mixstage::CTAS; }
 
 }  // namespace eb2

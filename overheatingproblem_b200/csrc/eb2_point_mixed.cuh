@@ -50,22 +50,81 @@ EB2_HD float rsq(float x) {
 }
 EB2_HD float sqr(float x) { return x * rsq(x); }  // sqrt for x > 0
 
+// --- two-lane arithmetic -----------------------------------------------------
+// The two sides of an interface run the same reconstruction on mirrored
+// stencils, so they ride the two lanes of one float2: .x the minus side
+// (around cell i), .y the plus side (around cell i+1).  On the GPU each
+// operation is one packed FP32 instruction of sm_100 (FFMA2 / FMUL2 / FADD2,
+// round to nearest), which halves the issue slots of the per-side arithmetic;
+// on the host (CPU checks of this file) it is two scalar operations with the
+// same rounding.
+using f2 = float2;
+EB2_HD f2 f2s(float a) { return make_float2(a, a); }
+EB2_HD f2 f2n(f2 a) { return make_float2(-a.x, -a.y); }
+EB2_HD f2 fma2(f2 a, f2 b, f2 c) {
+#ifdef __CUDA_ARCH__
+    return __ffma2_rn(a, b, c);
+#else
+    return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+EB2_HD f2 mul2(f2 a, f2 b) {
+#ifdef __CUDA_ARCH__
+    return __fmul2_rn(a, b);
+#else
+    return make_float2(a.x * b.x, a.y * b.y);
+#endif
+}
+EB2_HD f2 add2(f2 a, f2 b) {
+#ifdef __CUDA_ARCH__
+    return __fadd2_rn(a, b);
+#else
+    return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+EB2_HD f2 sub2(f2 a, f2 b) { return add2(a, f2n(b)); }
+EB2_HD f2 rcp2(f2 a) { return make_float2(rcp(a.x), rcp(a.y)); }
+// the bits of a float (zero tests without floating-point compares)
+EB2_HD unsigned bits(float x) {
+#ifdef __CUDA_ARCH__
+    return __float_as_uint(x);
+#else
+    unsigned u;
+    memcpy(&u, &x, sizeof u);
+    return u;
+#endif
+}
+
+// 1/x for a positive normal double to ~1e-17 relative: the SFU seed refined by
+// one third-order Newton-Raphson step, y (1 + e + e^2) with e = 1 - x y.
+EB2_HD double rcp64(double x) {
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+#else
+    return 1.0 / x;
+#endif
+}
+
 // Per-cell primitive data kept in shared memory (FP32 values of FP64 results).
 enum : int { P_RHO = 0, P_U = 1, P_V = 2, P_P = 3, P_H = 4, P_SR = 5, NP = 6 };
 
-// Primitive record of one cell from its FP64 conserved state: the pressure is
-// formed in FP64 (E - kinetic cancels in low-pressure flows), then stored FP32.
-EB2_HD void cell_prims(const double* q, const Gas& g, float* P, int ps) {
-    double rho = q[0];
-    double ir = 1.0 / rho;
-    double uu = q[1] * ir, vv = q[2] * ir;
-    double p = (q[3] - 0.5 * (q[1] * uu + q[2] * vv)) * g.gm1;
-    P[P_RHO * ps] = (float)rho;
-    P[P_U * ps] = (float)uu;
-    P[P_V * ps] = (float)vv;
-    P[P_P * ps] = (float)p;
-    P[P_H * ps] = (float)(g.gr * p * ir);
-    P[P_SR * ps] = (float)sqrt(rho);
+// Primitive record of one cell from its conserved state (q in FP64, qf the
+// same values rounded to FP32): the pressure is formed in FP64, where E minus
+// the kinetic energy cancels in low-pressure flows, then stored FP32; the
+// velocities, enthalpy and sqrt(rho) need only FP32.
+EB2_HD void cell_prims(const double* q, const float* qf, const Gas& g, float* P, int ps) {
+    const double ir = rcp64(q[0]);
+    const double p = fma(-0.5 * ir, fma(q[1], q[1], q[2] * q[2]), q[3]) * g.gm1;
+    const float pf = (float)p, irf = rcp(qf[0]);
+    P[P_RHO * ps] = qf[0];
+    P[P_U * ps] = qf[1] * irf;
+    P[P_V * ps] = qf[2] * irf;
+    P[P_P * ps] = pf;
+    P[P_H * ps] = (float)g.gr * pf * irf;
+    P[P_SR * ps] = sqr(qf[0]);
 }
 
 // Eigen-system parameters at an interface (the Roe average), in the form the
@@ -243,6 +302,76 @@ EB2_HD void weno5_pair(float w0, float w1, float w3, float w4, float w5,
     qp = side(bR1, bR2, bR3, cr1, cr2, cr3);
 }
 
+// WENO5 of both sides of an interface in the two lanes, from the characteristic
+// differences y_n = w_n - w_i of cells n = i-2..i+3 (y2 = 0).  The plus side is
+// WENO5_R on i-1..i+3, which is WENO5_L on the mirrored stencil i+3..i-1; taken
+// relative to its own base cell i+1 it reads (y5-y3, y4-y3, 0, -y3, y1-y3).  So
+// one evaluation of the left-biased formulas on the lane pairs
+//   X0 = (y0, y5-y3), X1 = (y1, y4-y3), X3 = (y3, -y3), X4 = (y4, y1-y3)
+// gives the minus-side value relative to cell i in .x and the plus-side value
+// relative to cell i+1 in .y (Reconstruction.h:1408-1508 for the JS weights,
+// :1519-1624 for WENO-Z).  A flat upwind side returns its own cell's state
+// exactly, as the FP64 form does.
+//
+// The smoothness indicators are carried as t_k = 12/13 (beta_k + eps) =
+// a_k^2 + 3/13 b_k^2 + 12/13 eps: the weights depend only on ratios of the
+// t_k (and, for WENO-Z, of tau5 = |t1 - t3| to t_k), so the common factor
+// drops out and saves one multiply per indicator.  eps is the reference's
+// absolute 1e-15.  The weights are SFU reciprocals of t (t >= 1e-15, so 1/t
+// stays below 1e15); the floor on their sum only keeps a stencil whose three
+// weights all flush to zero (values beyond ~1e9) finite.
+template <bool WZ>
+EB2_HD f2 weno5_lanes(f2 X0, f2 X1, f2 X3, f2 X4) {
+    const f2 m2 = f2s(-2.0f), m4 = f2s(-4.0f);
+    const f2 a1 = fma2(X1, m2, X0), b1 = fma2(X1, m4, X0);   // w0-2w1+w2, w0-4w1+3w2
+    const f2 a2 = add2(X1, X3), b2 = sub2(X1, X3);           // w1-2w2+w3, w1-w3
+    const f2 a3 = fma2(X3, m2, X4), b3 = fma2(X3, m4, X4);   // w2-2w3+w4, 3w2-4w3+w4
+    const f2 k = f2s(3.0f / 13.0f), e = f2s(12.0f / 13.0f * 1.0e-15f);
+    const f2 t1 = fma2(a1, a1, fma2(mul2(k, b1), b1, e));
+    const f2 t2 = fma2(a2, a2, fma2(mul2(k, b2), b2, e));
+    const f2 t3 = fma2(a3, a3, fma2(mul2(k, b3), b3, e));
+    // candidate values times 6 relative to the base (Reconstruction.h:1452-1454)
+    const f2 c1 = fma2(X1, f2s(-7.0f), add2(X0, X0));        // 2w0 - 7w1 + 11w2
+    const f2 c2 = fma2(X3, f2s(2.0f), f2n(X1));              // -w1 + 5w2 + 2w3
+    const f2 c3 = fma2(X3, f2s(5.0f), f2n(X4));              // 2w2 + 5w3 - w4
+    const f2 r1 = rcp2(t1), r2 = rcp2(t2), r3 = rcp2(t3);
+    f2 g1, g2, g3;
+    if (WZ) {
+        const f2 d = sub2(t1, t3);
+        const f2 tau = make_float2(fabsf(d.x), fabsf(d.y));
+        g1 = fma2(mul2(tau, r1), f2s(0.1f), f2s(0.1f));
+        g2 = fma2(mul2(tau, r2), f2s(0.6f), f2s(0.6f));
+        g3 = fma2(mul2(tau, r3), f2s(0.3f), f2s(0.3f));
+    } else {
+        g1 = mul2(mul2(r1, f2s(0.1f)), r1);
+        g2 = mul2(mul2(r2, f2s(0.6f)), r2);
+        g3 = mul2(mul2(r3, f2s(0.3f)), r3);
+    }
+    const f2 s = add2(add2(g1, g2), g3);
+    const f2 rs = mul2(rcp2(make_float2(fmaxf(s.x, 0x1p-126f), fmaxf(s.y, 0x1p-126f))),
+                       f2s(1.0f / 6.0f));
+    return mul2(fma2(g1, c1, fma2(g2, c2, mul2(g3, c3))), rs);
+}
+
+// Conserved differences of both sides from their characteristic values (the
+// right eigenvectors of unproject, Characteriz.h:371-392 / :473-494), lane by
+// lane.
+template <int DIR>
+EB2_HD void unproject2(const Eig& e, const f2* w, f2* q) {
+    const f2 S = fma2(f2s(e.b1), w[1], add2(w[0], w[3]));
+    const f2 cD = mul2(f2s(e.c), sub2(w[0], w[3]));
+    q[0] = S;
+    if (DIR == 1) {
+        q[1] = fma2(f2s(e.u), S, f2n(cD));
+        q[2] = fma2(f2s(e.v), S, f2n(w[2]));
+        q[3] = fma2(f2s(e.H), S, fma2(f2s(-e.u), cD, fma2(f2s(-e.v), w[2], f2n(w[1]))));
+    } else {
+        q[1] = fma2(f2s(e.u), S, w[2]);
+        q[2] = fma2(f2s(e.v), S, f2n(cD));
+        q[3] = fma2(f2s(e.H), S, fma2(f2s(-e.v), cD, fma2(f2s(e.u), w[2], f2n(w[1]))));
+    }
+}
+
 // Interface state in primitive form from the base cell and a conserved
 // difference (no cancellation: see the file comment).
 struct Prim {
@@ -269,6 +398,37 @@ EB2_HD Prim prim_from_delta(float rb, float ub, float vb, float pb, float Eb,
     s.un = DIR == 1 ? u : v;
     s.ut = DIR == 1 ? v : u;
     return s;
+}
+
+// prim_from_delta for both sides at once: lane .x from cell i and the
+// minus-side difference, lane .y from cell i+1 and the plus-side difference.
+template <int DIR>
+EB2_HD void prim_from_delta2(f2 rb, f2 ub, f2 vb, f2 pb, f2 Eb, const f2* dq, float gm1,
+                             Prim& L, Prim& R) {
+    const f2 r = add2(rb, dq[0]);
+    const f2 ir = rcp2(r);
+    const f2 u = fma2(fma2(f2n(ub), dq[0], dq[1]), ir, ub);
+    const f2 v = fma2(fma2(f2n(vb), dq[0], dq[2]), ir, vb);
+    // dK = [rb (2 ub.dm - drho |ub|^2) + |dm|^2] / (2 r)
+    const f2 udm = fma2(ub, dq[1], mul2(vb, dq[2]));
+    const f2 q2 = fma2(ub, ub, mul2(vb, vb));
+    const f2 t = fma2(rb, fma2(f2s(2.0f), udm, f2n(mul2(dq[0], q2))),
+                      fma2(dq[1], dq[1], mul2(dq[2], dq[2])));
+    const f2 dK = mul2(mul2(f2s(0.5f), t), ir);
+    const f2 p = fma2(f2s(gm1), sub2(dq[3], dK), pb);
+    const f2 E = add2(Eb, dq[3]);
+    L.r = r.x;
+    L.ir = ir.x;
+    L.p = p.x;
+    L.E = E.x;
+    L.un = DIR == 1 ? u.x : v.x;
+    L.ut = DIR == 1 ? v.x : u.x;
+    R.r = r.y;
+    R.ir = ir.y;
+    R.p = p.y;
+    R.E = E.y;
+    R.un = DIR == 1 ? u.y : v.y;
+    R.ut = DIR == 1 ? v.y : u.y;
 }
 
 // Physical flux in (mass, normal momentum, tangential momentum, energy) order.

@@ -18,6 +18,12 @@ namespace eb2 {
 namespace mixstage {
 
 constexpr int TX = MIXED_TILE_X, TY = STAGE_TILE_Y, NT = 256;
+// CTAs of the stage kernel resident per SM (the register budget follows:
+// 65536 / (NT * CTAS) per thread)
+#ifndef EB2_MIXED_CTAS
+#define EB2_MIXED_CTAS 4
+#endif
+constexpr int CTAS = EB2_MIXED_CTAS;
 constexpr int HX = TX + 6, HY = TY + 6;
 constexpr int PX = TX + 2, PY = TY + 2;
 constexpr int FS = HX * HY;
@@ -55,35 +61,45 @@ EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
     }
     const float b0 = s[2 * stride], b1 = s[FS + 2 * stride], b2 = s[2 * FS + 2 * stride],
                 b3 = s[3 * FS + 2 * stride];
-    float w[4][6];
+    // characteristic differences y_n = L (U_n - U_i), n = i-2..i+3 (y_2 = 0)
+    float y[4][6];
 #pragma unroll
     for (int n = 0; n < 6; n++) {
-        if (n == 2) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) w[k][2] = 0.0f;
-            continue;
-        }
+        if (n == 2) continue;
         float d0 = s[n * stride] - b0, d1 = s[FS + n * stride] - b1;
         float d2 = s[2 * FS + n * stride] - b2, d3 = s[3 * FS + n * stride] - b3;
         float c[4];
         f32::project<DIR>(e, d0, d1, d2, d3, c);
 #pragma unroll
-        for (int k = 0; k < 4; k++) w[k][n] = c[k];
+        for (int k = 0; k < 4; k++) y[k][n] = c[k];
     }
-    float wm[4], wp[4];
+    // both sides of each field in the two lanes (weno5_lanes); a field whose
+    // stencil is flat on both sides reconstructs its base values exactly, and
+    // uniform regions, where whole warps agree, skip the weights
+    f32::f2 W[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
-        f32::weno5_pair<WZ>(w[k][0], w[k][1], w[k][3], w[k][4], w[k][5], wm[k], wp[k]);
-    float dqm[4], dqp[4];
-    f32::unproject<DIR>(e, wm, dqm);
-    f32::unproject<DIR>(e, wp, dqp);
+    for (int k = 0; k < 4; k++) {
+        const unsigned any = (f32::bits(y[k][0]) | f32::bits(y[k][1]) | f32::bits(y[k][3]) |
+                              f32::bits(y[k][4]) | f32::bits(y[k][5])) << 1;
+        if (any == 0u) {
+            W[k] = f32::f2s(0.0f);
+        } else {
+            const float y3 = y[k][3];
+            W[k] = f32::weno5_lanes<WZ>(make_float2(y[k][0], y[k][5] - y3),
+                                        make_float2(y[k][1], y[k][4] - y3), make_float2(y3, -y3),
+                                        make_float2(y[k][4], y[k][1] - y3));
+        }
+    }
+    f32::f2 dq[4];
+    f32::unproject2<DIR>(e, W, dq);
     // minus side around cell i, plus side around cell i+1
     const float ra = pa[f32::P_RHO * PS], ua = pa[f32::P_U * PS], va = pa[f32::P_V * PS],
                 pas = pa[f32::P_P * PS];
     const float rb = pb[f32::P_RHO * PS], ub = pb[f32::P_U * PS], vb = pb[f32::P_V * PS],
                 pbs = pb[f32::P_P * PS], eb = s[3 * FS + 3 * stride];
-    f32::Prim L = f32::prim_from_delta<DIR>(ra, ua, va, pas, b3, dqm, gm1);
-    f32::Prim R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, eb, dqp, gm1);
+    f32::Prim L, R;
+    f32::prim_from_delta2<DIR>(make_float2(ra, rb), make_float2(ua, ub), make_float2(va, vb),
+                               make_float2(pas, pbs), make_float2(b3, eb), dq, gm1, L, R);
     unsigned st = 0;
     if (!(L.r > 0.0f && L.p > 0.0f && R.r > 0.0f && R.p > 0.0f)) {
         if (positivity) {
@@ -129,20 +145,35 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     const Gas g = a.gas;
     const float pthr = (float)(1.0e-3 * ctrl->pmean);
 
-    // 1. tile + halo as FP32; primitives of the tile and its first ring from FP64
-    for (int e = threadIdx.x; e < FS; e += NT) {
-        int r = e / HY, c = e - r * HY;
-        int i = i0 - 3 + r, j = j0 - 3 + c;
-        double q[4] = {0.0, 0.0, 0.0, 0.0};
-        if (i < rows && j < cols) {
-            size_t o = (size_t)i * cols + j;
+    // 1. tile + halo as FP32; primitives of the tile and its first ring from FP64.
+    // Thread t takes elements t, t + NT, ... of the HX x HY tile, its (row,
+    // column) stepped without divisions.
+    {
+        int r = threadIdx.x / HY, c = threadIdx.x - r * HY;
+        for (int e = threadIdx.x; e < FS; e += NT) {
+            const int i = i0 - 3 + r, j = j0 - 3 + c;
+            double q[4] = {0.0, 0.0, 0.0, 0.0};
+            if (i < rows && j < cols) {
+                const double* src = uin + (size_t)i * cols + j;
 #pragma unroll
-            for (int k = 0; k < 4; k++) q[k] = uin[o + k * plane];
+                for (int k = 0; k < 4; k++) q[k] = src[k * plane];
+            }
+            float qf[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                qf[k] = (float)q[k];
+                sU[k * FS + e] = qf[k];
+            }
+            const int pr = r - 2, pc = c - 2;
+            if ((unsigned)pr < (unsigned)PX && (unsigned)pc < (unsigned)PY)
+                f32::cell_prims(q, qf, g, sP + pr * PY + pc, PS);
+            c += NT % HY;
+            r += NT / HY;
+            if (c >= HY) {
+                c -= HY;
+                r++;
+            }
         }
-#pragma unroll
-        for (int k = 0; k < 4; k++) sU[k * FS + e] = (float)q[k];
-        int pr = r - 2, pc = c - 2;
-        if (pr >= 0 && pr < PX && pc >= 0 && pc < PY) f32::cell_prims(q, g, sP + pr * PY + pc, PS);
     }
     __syncthreads();
 
@@ -258,7 +289,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
 
 // Single solve: one CTA per tile.
 template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(NT, 4) k_stage(StageArgs a) {
+__global__ void __launch_bounds__(NT, CTAS) k_stage(StageArgs a) {
     stage_tile<WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
 }
 

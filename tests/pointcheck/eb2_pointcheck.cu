@@ -32,7 +32,9 @@ unsigned mixed_face(const double* cells, double pthr, const Gas& g, int pos, dou
         for (int k = 0; k < 4; k++) sU[k * mixstage::FS + n] = (float)cells[4 * n + k];
     double u[8];
     for (int c = 0; c < 2; c++) {
-        f32::cell_prims(cells + 4 * (2 + c), g, sP + c, mixstage::PS);
+        float qf[4];
+        for (int k = 0; k < 4; k++) qf[k] = (float)cells[4 * (2 + c) + k];
+        f32::cell_prims(cells + 4 * (2 + c), qf, g, sP + c, mixstage::PS);
         for (int k = 0; k < 4; k++) u[c + 2 * k] = cells[4 * (2 + c) + k];
     }
     float Ff[4];
