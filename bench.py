@@ -6,7 +6,9 @@ Workload (one step = one SSP-RK3 step of the whole grid, CFL time step from the
 device reduction): the four-quadrant Riemann problem on [0,1]^2, 1024 x 1024
 cells, gamma 1.4, characteristic WENO5-JS + HLLC + SSP-RK3, CFL 0.5, plain
 FP64 drop-in form (bit-identical to the reference).  Inputs are synthetic (the
-benchmark's own initial state); nothing is downloaded.
+benchmark's own initial state); nothing is downloaded.  Every timed window
+starts from the state advanced, untimed, to t = 0.15 (mid-run: the quadrants'
+waves have rolled up and few stencils are still uniform).
 
 Our arm prints one JSON line with
   value     cell-updates/s over all ranks, device time (CUDA events) of K
@@ -18,18 +20,23 @@ Our arm prints one JSON line with
             eb2_download);
   roofline  algorithmic HBM bytes of the fused stage kernel (256 B per cell per
             RK3 step: 64 + 96 + 96) over its measured device time, against the
-            measured copy bandwidth;
+            measured copy bandwidth; beside it the counted FP64/FP32 operations
+            per cell-stage against the same kernel's time;
   cpu_baseline  the reference built from its own sources (oracle/_ref), all
             host cores, on a bounded sample of the same workload;
-  extra     the same device-time measurement for the 4096^2 grid in the FP64
-            and mixed-precision forms (HLLC and Roe).
+  extra     (one GPU) whole runs to t = 0.3 and mid-run windows of the 1024^2
+            and 4096^2 grids in the FP64 and mixed forms (HLLC; Roe), the
+            mixed form's error against the FP64 form at every checkpoint with
+            the FP32-sized floor of the flow itself, and the served stream of
+            512 requests (batched mixed server against one-at-a-time mixed and
+            one-at-a-time plain FP64 solves).
 With --impl reference, rank 0 times the reference's CPU implementation on the
 same workload and prints the reference line; other ranks exit.
 For N > 1 (torchrun) every rank runs an independent replica (weak scaling):
 a single solve of this size does not shard in this build.
 
 --nx/--precision/--scheme/--no-e2e/--no-cpu-baseline/--no-extra select a single
-measurement (used for profiling runs).
+measurement (used for profiling runs); --serve N runs only the served stream.
 """
 from __future__ import annotations
 
@@ -68,9 +75,8 @@ def parse():
     ap.add_argument("--serve", type=int, default=None, metavar="N",
                     help="served stream of N requests only (batched vs one-at-a-time)")
     ap.add_argument("--serve-rate", type=float, default=20.0)
-    ap.add_argument("--serve-baseline", type=int, default=None,
-                    help="time only the first N requests one at a time in FP64 "
-                         "(default: the whole stream, the same requests as the server)")
+    ap.add_argument("--serve-requests", type=int, default=512,
+                    help="requests of the served stream in the default line (0: none)")
     ap.add_argument("--dmr", action="store_true",
                     help="double Mach reflection 1920x480 to t = 0.2, FP64 and mixed")
     ap.add_argument("--accuracy", type=float, default=None, metavar="T",
@@ -107,113 +113,270 @@ def stream_trace(n, rate, seed, eb2):
     return reqs, arrivals
 
 
-def serve_stream(eb2, local, n, rate, seed, baseline_n, reps=3):
-    """Batched mixed-precision server vs one-at-a-time plain FP64 solves on the
-    same trace: solves/s and latency percentiles (finish - arrival); the server
-    side is the median of `reps` replays."""
+def one_at_a_time(eb2, local, reqs, arr, precision, sample):
+    """Each request on its own context, started when it has arrived and the
+    previous one has finished (one solve on the GPU at a time); the final
+    states of the `sample` requests are kept."""
+    import numpy as np
+    t0 = time.perf_counter()
+    fin = np.zeros(len(reqs))
+    status = np.zeros(len(reqs), dtype=np.uint32)
+    kept = {}
+    for i, r in enumerate(reqs):
+        wait = arr[i] - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        with eb2.Solver(r.nx, r.ny, device=local, recon=5, characteristic=True, weno_z=False,
+                        cfl=r.cfl, precision=precision) as s:
+            lx, ly, _ = s.init_case(r.test_case, r.q)
+            ly = r.ly if r.ly > 0 else ly
+            s.run(ORDER, 2, lx / r.nx, ly / r.ny, r.tmax)
+            U = s.download()
+            status[i] = s.status()
+        if i in sample:
+            kept[i] = U
+        fin[i] = time.perf_counter() - t0
+    return fin, status, kept
+
+
+def arm_summary(n, makespan, lat, status):
+    import numpy as np
+    bad = [int(i) for i in np.nonzero(status)[0]]
+    return {"solves_per_s": n / makespan, "makespan_s": float(makespan),
+            "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "requests": n,
+            "non_physical": len(bad), "non_physical_ids": bad,
+            "physical_solves_per_s": (n - len(bad)) / makespan}
+
+
+def serve_stream(eb2, local, n, rate, seed, reps=1, nsample=16):
+    """The batched mixed-precision server against one-at-a-time mixed and
+    one-at-a-time plain FP64 solves on the same trace: solves/s (all, and the
+    solves that stayed physical), latency percentiles (finish - arrival), the
+    requests that went non-physical by id, and the density error of the
+    server's results against the one-at-a-time FP64 results on a sample of
+    requests."""
     import numpy as np
 
     from overheatingproblem_b200.server import Server
     reqs, arr = stream_trace(n, rate, seed, eb2)
-    # The trace is replayed in real time, so how requests meet in batches (and the
-    # rate) varies from replay to replay: three replays, the median one reported.
+    sample = set(range(0, n, max(1, n // nsample)))
+    # The trace is replayed in real time, so how requests meet in batches (and
+    # the rate) varies from replay to replay; with reps > 1 the median replay
+    # is reported and all are listed.
     runs = []
     with Server(device=local, precision=eb2.lib.MIXED, scheme=2,
                 hbm_budget=120 * 10**9) as srv:
         for _ in range(reps):
-            runs.append(srv.run_trace(reqs, arr))
-    runs.sort(key=lambda o: o["makespan"])
-    out = runs[len(runs) // 2]
-    lat = out["finish"] - arr
-    batched = {"solves_per_s": n / out["makespan"], "makespan_s": out["makespan"],
-               "p50_latency_s": float(np.percentile(lat, 50)),
-               "p99_latency_s": float(np.percentile(lat, 99)), "requests": n,
-               "steps": int(out["steps"].sum()),
-               "non_physical": int((out["status"] != 0).sum()),
-               "replays_solves_per_s": [n / o["makespan"] for o in runs]}
-    # one-at-a-time plain FP64 launches: each request on its own context,
-    # started when it has arrived and the previous one has finished
-    m = n if baseline_n is None else min(baseline_n, n)
-    t0 = time.perf_counter()
-    fin = np.zeros(m)
-    bad = 0
-    for i in range(m):
-        wait = arr[i] - (time.perf_counter() - t0)
-        if wait > 0:
-            time.sleep(wait)
-        r = reqs[i]
-        with eb2.Solver(r.nx, r.ny, device=local, recon=5, characteristic=True, weno_z=False,
-                        cfl=r.cfl, precision=eb2.lib.FP64) as s:
-            lx, ly, _ = s.init_case(r.test_case, r.q)
-            ly = r.ly if r.ly > 0 else ly
-            s.run(ORDER, 2, lx / r.nx, ly / r.ny, r.tmax)
-            s.download()
-            bad += s.status() != 0
-        fin[i] = time.perf_counter() - t0
-    blat = fin - arr[:m]
-    base = {"solves_per_s": m / fin[-1], "makespan_s": float(fin[-1]),
-            "p50_latency_s": float(np.percentile(blat, 50)),
-            "p99_latency_s": float(np.percentile(blat, 99)), "requests": m,
-            "non_physical": int(bad)}
+            runs.append(srv.run_trace(reqs, arr, keep_results=sample))
+    order = sorted(range(reps), key=lambda k: runs[k]["makespan"])
+    out = runs[order[len(order) // 2]]
+    batched = arm_summary(n, out["makespan"], out["finish"] - arr, out["status"])
+    batched["steps"] = int(out["steps"].sum())
+    batched["replays_solves_per_s"] = [n / o["makespan"] for o in runs]
+    fin_m, st_m, _ = one_at_a_time(eb2, local, reqs, arr, eb2.lib.MIXED, set())
+    mixed1 = arm_summary(n, fin_m[-1], fin_m - arr, st_m)
+    fin_d, st_d, kept = one_at_a_time(eb2, local, reqs, arr, eb2.lib.FP64, sample)
+    fp641 = arm_summary(n, fin_d[-1], fin_d - arr, st_d)
+    err = []
+    for i in sorted(sample):
+        if st_d[i] or out["status"][i]:
+            continue
+        a = kept[i][0, 4:-4, 4:-4]
+        b = out["results"][i][0, 4:-4, 4:-4]
+        d = np.abs(a - b)
+        err.append({"request": i, "n": reqs[i].nx, "t_final": reqs[i].tmax,
+                    "l1_rho": float(d.mean()), "linf_rho": float(d.max()),
+                    "rel_l1_rho": float(d.sum() / np.abs(a).sum())})
+    acc = {"vs": "one-at-a-time FP64 results of the same requests (density; L1 = mean "
+                 "|d rho| over the cells, Linf = max)",
+           "sample": err,
+           "max_l1_rho": max((e["l1_rho"] for e in err), default=None),
+           "median_l1_rho": float(np.median([e["l1_rho"] for e in err])) if err else None}
     return {"trace": f"{n} requests, Poisson arrivals at {rate}/s, seed {seed}",
-            "batched_mixed": batched, "one_at_a_time_fp64": base,
-            "speedup_solves_per_s": batched["solves_per_s"] / base["solves_per_s"]}
+            "batched_mixed": batched, "one_at_a_time_mixed": mixed1,
+            "one_at_a_time_fp64": fp641,
+            "speedup_solves_per_s": batched["solves_per_s"] / fp641["solves_per_s"],
+            "speedup_vs_one_at_a_time_mixed": batched["solves_per_s"] / mixed1["solves_per_s"],
+            "accuracy": acc}
+
+
+MARKS = (0.05, 0.1, 0.15, 0.2, 0.25, 0.3)   # checkpoints of the whole runs
+T_START = 0.15                               # every timed window starts here
+L1_BOUND = 1e-6                              # the density L1 bound of the mixed form
+
+
+def four_quadrant(eb2, local, n, precision):
+    prec = eb2.lib.FP64 if precision == "fp64" else eb2.lib.MIXED
+    s = eb2.Solver(n, n, device=local, recon=5, characteristic=True, weno_z=False, cfl=0.5,
+                   precision=prec)
+    lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
+    return s, lx / n, ly / n
+
+
+def fp32_perturbation(seed):
+    """Every interior value of the initial state moved by a seeded relative
+    2^-24 up or down: rounding of FP32 size applied everywhere once."""
+    import numpy as np
+
+    def apply(U):
+        rng = np.random.default_rng(seed)
+        inner = U[:, 4:-4, 4:-4]
+        inner *= 1.0 + rng.choice([-1.0, 1.0], size=inner.shape) * 2.0 ** -24
+    return apply
+
+
+def whole_run(eb2, local, n, precision, scheme, marks=MARKS, perturb=None, save_at=None):
+    """The four-quadrant problem run to marks[-1] by the device time loop
+    (eb2_run), paused at every mark (the CFL step is clipped there, in every
+    run alike) to record the density; the final primitives; the conserved
+    state at `save_at`.  Seconds are those of the device loop segments."""
+    s, dx, dy = four_quadrant(eb2, local, n, precision)
+    if perturb is not None:
+        U = s.download()
+        perturb(U)
+        s.upload(U)
+    t, steps, el, rho, saved, pri = 0.0, 0, 0.0, [], None, None
+    for tm in marks:
+        t0 = time.perf_counter()
+        k, t = s.run(ORDER, scheme, dx, dy, tm, t0=t)
+        el += time.perf_counter() - t0
+        steps += k
+        pri = s.con_to_pri()
+        rho.append(pri[0, 4:-4, 4:-4].copy())
+        if save_at is not None and abs(tm - save_at) < 1e-12:
+            saved = s.download()
+    info = {"steps": steps, "t_final": t, "seconds": el, "status_flags": s.status(),
+            "cell_updates_per_s": n * n * steps / el}
+    return s, dx, dy, info, rho, pri[:, 4:-4, 4:-4].copy(), saved
+
+
+def compare(ref, got, marks=MARKS):
+    """Differences of a run against the reference run (FP64): density L1
+    (mean |d rho| over the cells, i.e. dx dy sum |d rho| on the unit square,
+    the norm of include/Error.h:129-160) and Linf at every checkpoint, all
+    four primitives at the final time, and the last checkpoint up to which
+    the density L1 stays within 1e-6."""
+    import numpy as np
+    (rho_a, fin_a), (rho_b, fin_b) = ref, got
+    cps = []
+    for tm, a, b in zip(marks, rho_a, rho_b):
+        d = np.abs(a - b)
+        cps.append({"t": tm, "l1_rho": float(d.mean()), "linf_rho": float(d.max())})
+    last = None
+    for c in cps:
+        if c["l1_rho"] > L1_BOUND:
+            break
+        last = c["t"]
+    d = np.abs(fin_a - fin_b)
+    names = ["rho", "u", "v", "p"]
+    return {"t_final": marks[-1], "l1": {q: float(d[i].mean()) for i, q in enumerate(names)},
+            "linf": {q: float(d[i].max()) for i, q in enumerate(names)},
+            "rel_l1_rho": float(d[0].sum() / np.abs(fin_a[0]).sum()), "checkpoints": cps,
+            "last_t_with_l1_rho_le_1e-6": last}
+
+
+def window(s, state, scheme, dx, dy, k, warmup=2):
+    """Device time of k steps from `state` (L2 flushed between steps), after
+    `warmup` untimed steps from the same state."""
+    s.upload(state)
+    if warmup:
+        s.bench_steps(ORDER, scheme, dx, dy, warmup, 0)
+        s.upload(state)
+    step_ms, stage_ms, nstage, launches = s.bench_steps(ORDER, scheme, dx, dy, k, FLUSH_BYTES)
+    return step_ms, stage_ms, nstage, launches, s.status()
+
+
+def window_entry(n, k, step_ms, stage_ms, nstage, st, peak, whole=None):
+    tot = float(sum(step_ms))
+    e = {"value": n * n * k / (tot * 1e-3), "unit": METRIC, "ms_per_step": tot / k, "steps": k,
+         "start": f"t = {T_START} (advanced untimed), L2 flushed between steps",
+         "status_flags": st,
+         "roofline_frac": n * n * BYTES_PER_CELL_STEP * k / (stage_ms * 1e-3) / 1e9 / peak,
+         "step_roofline_frac": n * n * BYTES_PER_CELL_STEP * k / (tot * 1e-3) / 1e9 / peak,
+         "stage_ms": stage_ms / nstage}
+    if whole is not None:
+        e["whole_run"] = whole
+    return e
+
+
+def short_accuracy(acc):
+    return {"vs": "FP64 form", "t_final": acc["t_final"], "l1_rho": acc["l1"]["rho"],
+            "linf_rho": acc["linf"]["rho"], "rel_l1_rho": acc["rel_l1_rho"],
+            "last_t_with_l1_rho_le_1e-6": acc["last_t_with_l1_rho_le_1e-6"]}
+
+
+def run_extras(eb2, local, peak, rate, nserve):
+    """Whole runs, mid-run windows, accuracy and the served stream (one GPU)."""
+    extra, acc = {}, {}
+    # 1024^2: FP64 and mixed whole runs (HLLC, Roe), the FP32-sized floor
+    for name, sch in (("hllc", 2), ("roe", 3)):
+        s64, dx, dy, i64, r64, f64, _ = whole_run(eb2, local, 1024, "fp64", sch)
+        s64.close()
+        sm, dx, dy, im, rm, fm, um = whole_run(eb2, local, 1024, "mixed", sch, save_at=T_START)
+        a = compare((r64, f64), (rm, fm))
+        if sch == 2:
+            extra["fp64_1024_hllc_whole_run"] = i64
+            w = window(sm, um, sch, dx, dy, 200)
+            extra["mixed_1024_hllc"] = window_entry(1024, 200, *w[:3], w[4], peak, im)
+            extra["mixed_1024_hllc"]["accuracy"] = short_accuracy(a)
+            sp, _, _, ip, rp, fp, _ = whole_run(eb2, local, 1024, "fp64", sch,
+                                                perturb=fp32_perturbation(11))
+            sp.close()
+            a["floor_fp32_perturbed_fp64"] = compare((r64, f64), (rp, fp))["checkpoints"]
+        else:
+            extra["mixed_1024_roe_whole_run"] = im
+            extra["mixed_1024_roe_whole_run"]["accuracy"] = short_accuracy(a)
+        acc[f"four_quadrant_1024_{name}"] = a
+        sm.close()
+    # 4096^2: the FP64 HLLC run is the accuracy reference of the mixed HLLC run
+    s64, dx, dy, i64, r64, f64, u64 = whole_run(eb2, local, 4096, "fp64", 2, save_at=T_START)
+    w = window(s64, u64, 2, dx, dy, 10)
+    extra["fp64_4096_hllc"] = window_entry(4096, 10, *w[:3], w[4], peak, i64)
+    s64.close()
+    del u64
+    for name, sch in (("hllc", 2), ("roe", 3)):
+        sm, dx, dy, im, rm, fm, um = whole_run(eb2, local, 4096, "mixed", sch, save_at=T_START)
+        w = window(sm, um, sch, dx, dy, 40)
+        extra[f"mixed_4096_{name}"] = window_entry(4096, 40, *w[:3], w[4], peak, im)
+        if sch == 2:
+            a = compare((r64, f64), (rm, fm))
+            acc["four_quadrant_4096_hllc"] = a
+            extra["mixed_4096_hllc"]["accuracy"] = short_accuracy(a)
+        else:
+            extra["mixed_4096_roe"]["accuracy"] = dict(
+                short_accuracy(acc["four_quadrant_1024_roe"]),
+                note="measured at 1024^2 (four_quadrant_1024_roe): an FP64 Roe run at 4096^2 "
+                     "would add three minutes")
+        sm.close()
+        del um, rm, fm
+    del r64, f64
+    if nserve:
+        extra["served_stream"] = serve_stream(eb2, local, nserve, rate, 7)
+    return extra, acc
 
 
 def run_accuracy(args, local):
-    """FP64 vs mixed on the benchmark problem up to t = T, with checkpoints:
-    density/velocity/pressure L1 (mean over cells) and Linf differences.  A
-    third run, FP64 from the same initial state with one density value moved
-    by one ulp, measures how far the flow itself amplifies a perturbation of
-    rounding size (the floor no arithmetic can go below)."""
-    import numpy as np
-    import torch
-
+    """FP64 vs mixed on the benchmark problem up to t = T with checkpoints,
+    and the FP64 run from an initial state perturbed by a relative 2^-24 in
+    every value (the floor the flow's own amplification sets for any
+    arithmetic of FP32 size)."""
     import overheatingproblem_b200 as eb2
 
     nx, scheme, T = args.nx, SCHEMES[args.scheme], args.accuracy
-    marks = [t for t in (0.05, 0.1, 0.2) if t < T] + [T]
-    runs = {"fp64": eb2.lib.FP64, "mixed": eb2.lib.MIXED, "fp64_1ulp": eb2.lib.FP64}
-    out, prim = {}, {}
-    for name, prec in runs.items():
-        s = eb2.Solver(nx, nx, device=local, recon=5, characteristic=True, weno_z=False,
-                       cfl=0.5, precision=prec)
-        lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
-        if name == "fp64_1ulp":
-            U = s.download()
-            c = 4 + nx // 3
-            U[0, c, c] = np.nextafter(U[0, c, c], np.inf)
-            s.upload(U)
-        torch.cuda.synchronize(local)
-        el, steps, t = 0.0, 0, 0.0
-        prim[name] = []
-        for tm in marks:
-            t0 = time.perf_counter()
-            n, t = s.run(ORDER, scheme, lx / nx, ly / nx, tm, t0=t)
-            el += time.perf_counter() - t0
-            steps += n
-            prim[name].append(s.con_to_pri()[:, 4:-4, 4:-4].copy())
-        out[name] = {"steps": steps, "t_final": t, "seconds": el, "status_flags": s.status(),
-                     "cell_updates_per_s": nx * nx * steps / el}
+    marks = tuple(t for t in MARKS if t < T) + (T,)
+    runs, res = {}, {}
+    for name, prec, pert in (("fp64", "fp64", None), ("mixed", "mixed", None),
+                             ("fp64_fp32_floor", "fp64", fp32_perturbation(11))):
+        s, _, _, info, rho, fin, _ = whole_run(eb2, local, nx, prec, scheme, marks, pert)
         s.close()
-    names = ["rho", "u", "v", "p"]
-
-    def diff(other):
-        rows = []
-        for k, tm in enumerate(marks):
-            d = np.abs(prim["fp64"][k] - prim[other][k])
-            rows.append({"t": tm, "l1": {q: float(d[i].mean()) for i, q in enumerate(names)},
-                         "linf": {q: float(d[i].max()) for i, q in enumerate(names)}})
-        return rows
-
-    mixed, ulp = diff("mixed"), diff("fp64_1ulp")
+        runs[name] = info
+        res[name] = (rho, fin)
     line = {"accuracy": workload(nx, "mixed", args.scheme) + f" vs FP64, t = {T}",
-            "l1": mixed[-1]["l1"], "linf": mixed[-1]["linf"],
-            "rel_l1_rho": float(np.abs(prim["fp64"][-1][0] - prim["mixed"][-1][0]).sum() /
-                                np.abs(prim["fp64"][-1][0]).sum()),
-            "checkpoints": {"mixed_vs_fp64": mixed, "fp64_1ulp_vs_fp64": ulp},
+            "mixed_vs_fp64": compare(res["fp64"], res["mixed"], marks),
+            "fp32_floor_vs_fp64": compare(res["fp64"], res["fp64_fp32_floor"], marks),
             "note": "checkpoint times clip the CFL step in all three runs alike",
-            "runs": out}
+            "runs": runs}
     print(json.dumps(line), flush=True)
 
 
@@ -283,6 +446,7 @@ def config(args):
             "ny": args.nx, "order": ORDER, "scheme": args.scheme.upper(),
             "reconstruction": "WENO5-JS characteristic", "cfl": 0.5,
             "precision": args.precision,
+            "window_start": f"t = {T_START}, advanced untimed from the initial state",
             "l2": "flushed between timed steps (256 MiB write outside the timed intervals)",
             "parallelism": "replicas"}
 
@@ -302,17 +466,13 @@ def measured_traffic(nx, precision, scheme):
     return None
 
 
-def measured_compute(precision):
-    """The binding on-chip limit of the stage kernel, from the committed ncu
-    summary profiles/stage_<precision>_2048.md (its "now" column): FP64 pipe
-    activity for the FP64 form, issue activity for the mixed form (fractions
-    of peak), or None."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                        f"stage_{precision}_2048.md")
-    row = "FP64 pipe active" if precision == "fp64" else "issue active"
+def profile_rows(precision):
+    """Rows of the committed ncu summary profiles/stage_<precision>_2048.md as
+    {metric: value of its "now" column}."""
+    path = os.path.join(ROOT, "profiles", f"stage_{precision}_2048.md")
+    rows, col = {}, None
     if not os.path.exists(path):
-        return None
-    col = None
+        return rows
     for line in open(path):
         if not line.startswith("|"):
             continue
@@ -320,15 +480,64 @@ def measured_compute(precision):
         if cells[0] == "metric":
             col = next((i for i, c in enumerate(cells) if c.startswith("now") or "(now)" in c),
                        None)
-        elif col is not None and cells[0].startswith(row) and len(cells) > col:
-            try:
-                frac = float(cells[col].split()[0]) / 100.0
-            except ValueError:
-                return None
-            return {"limit": "fp64 pipe" if precision == "fp64" else "instruction issue",
-                    "active_frac": frac,
-                    "source": f"profiles/stage_{precision}_2048.md (ncu, 2048^2 stage)"}
-    return None
+        elif col is not None and len(cells) > col:
+            rows[cells[0]] = cells[col]
+    return rows
+
+
+def gemm_tflops(local, dtype, n):
+    """Measured dense GEMM rate (cuBLAS through torch, TF32 off) of `dtype` on
+    this GPU: the compute peak the stage kernel's counted operations are set
+    against."""
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    dev = f"cuda:{local}"
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
+    for _ in range(2):
+        a @ b
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        a @ b
+    e1.record()
+    e1.synchronize()
+    return 5 * 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+
+def measured_compute(precision, cells, per_launch_ms, local):
+    """The stage kernel against its on-chip limits: the binding pipe from the
+    committed ncu summary (FP64 pipe for the FP64 form, instruction issue for
+    the mixed form), and the arithmetic per cell-stage counted there by ncu
+    (DADD/DMUL/DFMA and FADD/FMUL/FFMA plus the packed FADD2/FMUL2/FFMA2; an
+    FMA counts two operations, a packed instruction two lanes) over the live
+    per-launch time, against a measured GEMM rate of the same precision."""
+    rows = profile_rows(precision)
+    row = "FP64 pipe active" if precision == "fp64" else "issue active"
+    out = {"limit": "fp64 pipe" if precision == "fp64" else "instruction issue",
+           "source": f"profiles/stage_{precision}_2048.md (ncu, 2048^2 stage)"}
+    key = next((k for k in rows if k.startswith(row)), None)
+    try:
+        out["active_frac"] = float(rows[key].split()[0]) / 100.0 if key else None
+    except ValueError:
+        out["active_frac"] = None
+    for prec, dt, n in (("fp64", "float64", 8192), ("fp32", "float32", 8192)):
+        k = next((r for r in rows if r.startswith(f"{prec} operations per cell-stage")), None)
+        if k is None:
+            continue
+        try:
+            ops = float(rows[k].split()[0])
+        except ValueError:
+            continue
+        achieved = ops * cells / (per_launch_ms * 1e-3) / 1e12
+        entry = {"ops_per_cell_stage": ops, "achieved_tflops": achieved}
+        if local is not None:
+            import torch
+            peak = gemm_tflops(local, getattr(torch, dt), n)
+            entry.update(peak_tflops=peak, peak_kind=f"measured: cuBLAS {prec.upper()} GEMM "
+                         f"{n}^3 on this GPU", frac=achieved / peak)
+        out[prec] = entry
+    return out
 
 
 def hbm_peak():
@@ -489,21 +698,6 @@ def run_reference(args, world, rank):
 
 
 # --------------------------------------------------------------------------- GPU
-def measure(eb2, local, nx, precision, scheme, steps, warmup, flush=FLUSH_BYTES):
-    """Device time of `steps` steps (after `warmup`), L2 flushed between steps."""
-    prec = eb2.lib.FP64 if precision == "fp64" else eb2.lib.MIXED
-    s = eb2.Solver(nx, nx, device=local, recon=5, characteristic=True, weno_z=False, cfl=0.5,
-                   precision=prec)
-    lx, ly, _ = s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
-    dx, dy = lx / nx, ly / nx
-    if warmup:
-        s.bench_steps(ORDER, scheme, dx, dy, warmup, 0)
-        s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
-    step_ms, stage_ms, nstage, launches = s.bench_steps(ORDER, scheme, dx, dy, steps, flush)
-    st = s.status()
-    return s, dx, dy, step_ms, stage_ms, nstage, launches, st
-
-
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -512,15 +706,27 @@ def run_ours(args, world, rank, local):
 
     nx, scheme = args.nx, SCHEMES[args.scheme]
     torch.cuda.init()
-    # warm-up pass (clocks, kernel attributes) outside the timed region
-    s, *_ = measure(eb2, local, nx, args.precision, scheme, max(args.warmup, 3), 0, 0)
-    s.close()
+    # the state at t = T_START, advanced untimed; every step below starts there
+    s, dx, dy = four_quadrant(eb2, local, nx, args.precision)
+    s.run(ORDER, scheme, dx, dy, T_START)
+    state = s.download()
     torch.cuda.synchronize(local)
+    # clocks are sampled from the warm-up (at least ~1 s of steps, so that the
+    # sampler sees the GPU under load) through the timed steps
     sampler = ClockSampler(physical_gpu(local)) if rank == 0 else None
+    t_w = time.perf_counter()
+    nw = 0
+    while nw < max(args.warmup, 3) or time.perf_counter() - t_w < 1.0:
+        s.upload(state)
+        s.bench_steps(ORDER, scheme, dx, dy, max(args.warmup, 3), 0)
+        nw += max(args.warmup, 3)
+    s.upload(state)
+    torch.cuda.synchronize(local)
     barrier(world)
     torch.cuda.synchronize(local)
-    s, dx, dy, step_ms, stage_ms, nstage, launches, st = measure(
-        eb2, local, nx, args.precision, scheme, args.steps, 0)
+    step_ms, stage_ms, nstage, launches = s.bench_steps(ORDER, scheme, dx, dy, args.steps,
+                                                         FLUSH_BYTES)
+    st = s.status()
     torch.cuda.synchronize(local)
     barrier(world)
     clocks = sampler.stop() if sampler else None
@@ -538,18 +744,19 @@ def run_ours(args, world, rank, local):
                 "per_launch_ms": stage_ms / nstage, "peak_kind": peak_kind,
                 "alg_bytes_per_launch": nx * nx * BYTES_PER_CELL_STEP / ORDER,
                 "stage_share_of_step": stage_ms / sum(step_ms),
-                "compute": measured_compute(args.precision)}
+                "compute": measured_compute(args.precision, nx * nx, stage_ms / nstage,
+                                            local if rank == 0 else None)}
 
     e2e = None
     if not args.no_e2e:
-        s.init_case(eb2.lib.CASE_FOUR_QUADRANT)
         host = torch.empty((4, nx + 8, nx + 8), dtype=torch.float64, pin_memory=True).numpy()
-        s.download(host)
+        host[...] = state
         k_e2e = max(3, min(args.steps, 50))
         for _ in range(2):
             s.upload(host)
             s.rk_step(ORDER, scheme, s.delta_t(dx, dy), dx, dy)
             s.download(host)
+        host[...] = state
         barrier(world)
         t0 = time.perf_counter()
         for _ in range(k_e2e):
@@ -561,26 +768,13 @@ def run_ours(args, world, rank, local):
         e2e = {"value": world * nx * nx * k_e2e / e2e_s, "unit": "cell-updates/s",
                "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes) + 8,
                "steps": k_e2e, "timer": "host wall clock, max over ranks",
+               "start": f"t = {T_START}",
                "path": "eb2_upload + eb2_delta_t + eb2_rk_step + eb2_download"}
     s.close()
 
-    extra = {}
-    if not args.no_extra:
-        for tag, (n2, prec, sch, k) in {
-                "fp64_4096_hllc": (4096, "fp64", 2, 10),
-                "mixed_4096_hllc": (4096, "mixed", 2, 40),
-                "mixed_4096_roe": (4096, "mixed", 3, 40),
-                "mixed_1024_hllc": (1024, "mixed", 2, 200)}.items():
-            s2, _, _, sm, stm, nst, _, st2 = measure(eb2, local, n2, prec, sch, k, 2)
-            s2.close()
-            tot = allreduce_max(float(sum(sm)), world)
-            extra[tag] = {"value": world * n2 * n2 * k / (tot * 1e-3), "unit": "cell-updates/s",
-                          "ms_per_step": tot / k, "steps": k, "status_flags": st2,
-                          "roofline_frac": n2 * n2 * BYTES_PER_CELL_STEP * k / (stm * 1e-3) / 1e9
-                          / peak}
-        if rank == 0:
-            extra["served_stream"] = serve_stream(eb2, local, 64, args.serve_rate, 7,
-                                                  args.serve_baseline)
+    extra, accuracy = {}, None
+    if not args.no_extra and world == 1:
+        extra, accuracy = run_extras(eb2, local, peak, args.serve_rate, args.serve_requests)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -598,6 +792,8 @@ def run_ours(args, world, rank, local):
             "step_ms_min_median_max": [min(step_ms), float(np.median(step_ms)), max(step_ms)],
             "extra": extra,
         }
+        if accuracy is not None:
+            line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
 
 
@@ -615,8 +811,8 @@ def main():
         elif args.serve is not None:
             if rank == 0:
                 import overheatingproblem_b200 as eb2
-                print(json.dumps(serve_stream(eb2, local, args.serve, args.serve_rate, 7,
-                                              args.serve_baseline)), flush=True)
+                print(json.dumps(serve_stream(eb2, local, args.serve, args.serve_rate, 7)),
+                      flush=True)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

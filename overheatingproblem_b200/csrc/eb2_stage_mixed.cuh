@@ -11,7 +11,10 @@
 // weights).
 #pragma once
 
+#include <type_traits>
+
 #include "eb2_kernels.h"
+#include "eb2_point_fp64.cuh"
 #include "eb2_point_mixed.cuh"
 
 namespace eb2 {
@@ -35,63 +38,123 @@ constexpr int NJX = (TX + 1) * TY, NJY = TX * (TY + 1);
 // that flux differences telescope and the step conserves to FP64 round-off)
 constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS + 4 * XS + 4 * YS) * sizeof(float);
 
-// One interface.  s: stencil cell n = 0 of field 0 (fields FS apart, `stride`
-// along the sweep); pa/pb: primitive records of cells i and i+1 (fields PS
-// apart); ga/gb: the two cells in global memory (near-vacuum path).
-template <int DIR, bool WZ, int FLUX>
-EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
-                                                   const float* __restrict__ pa,
-                                                   const float* __restrict__ pb,
-                                                   const double* __restrict__ u, size_t ga,
-                                                   size_t gb, size_t plane, float pthr,
-                                                   const Gas& g, int positivity,
-                                                   float* __restrict__ out, int ostride) {
-    const float gm1 = (float)g.gm1, gamma = (float)g.gamma;
-    f32::Eig e;
-    if (pa[f32::P_P * PS] < pthr || pb[f32::P_P * PS] < pthr) {
-        double qa[4], qb[4];
+// Conserved differences of both sides of an interface next to a near-vacuum
+// cell: the stencil's six cells are read in FP64 from the stage input (cell i at
+// g2, cell i+1 at g2 + step), the Roe average and the left and right
+// eigenvector matrices are the reference's, in FP64 (Characteriz.h:333-392 for
+// x, :435-494 for y), and so are the projections of the differences onto them
+// and the back-projection; only the WENO weights and candidate values between
+// the two run in FP32 lanes, as on every other interface.  Rare, so kept out
+// of line: its FP64 arrays do not weigh on the registers of the common path.
+template <int DIR, bool WZ>
+__host__ __device__ __noinline__ void vacuum_delta(const double* __restrict__ u, size_t g2,
+                                          long long step, size_t plane, const Gas g,
+                                          f32::f2* dq) {
+    // the two cells next to the interface stay in registers; the other four
+    // are re-read per field (cache hits)
+    double qa[4], qb[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        qa[m] = u[g2 + m * plane];
+        qb[m] = u[g2 + step + m * plane];
+    }
+    double A[5], B[5];
+    x64::primitive5(qa[0], qa[1], qa[2], qa[3], g, A);
+    x64::primitive5(qb[0], qb[1], qb[2], qb[3], g, B);
+    const x64::Roe e = x64::roe_average(A, B, g.gm1);
+    // lane stencils of weno5_lanes: minus side relative to cell i (n = 0, 1, 3,
+    // 4), plus side mirrored and relative to cell i+1 (n = 5, 4, 2, 1)
+    const int nm[4] = {0, 1, 3, 4}, np[4] = {5, 4, 2, 1};
+    f32::f2 W[4];
+#pragma unroll 1
+    for (int k = 0; k < 4; k++) {
+        double l[4];
+        x64::left_row<DIR>(e, k, l);
+        f32::f2 X[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const size_t om = g2 + (nm[t] - 2) * step, op = g2 + (np[t] - 2) * step;
+            double xm = 0.0, xp = 0.0;
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                xm += l[m] * (u[om + m * plane] - qa[m]);
+                xp += l[m] * (u[op + m * plane] - qb[m]);
+            }
+            X[t] = make_float2((float)xm, (float)xp);
+        }
+        W[k] = f32::weno5_lanes<WZ>(X[0], X[1], X[2], X[3]);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        double r[4];
+        x64::right_row<DIR>(e, m, r);
+        double sm = 0.0, sp = 0.0;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            qa[k] = u[ga + k * plane];
-            qb[k] = u[gb + k * plane];
+            sm += r[k] * (double)W[k].x;
+            sp += r[k] * (double)W[k].y;
         }
-        e = f32::roe_f64(qa, qb, g.gm1, g.gr);
-    } else {
-        e = f32::roe_f32(pa, pb, PS, gm1);
+        dq[m] = make_float2((float)sm, (float)sp);
     }
-    const float b0 = s[2 * stride], b1 = s[FS + 2 * stride], b2 = s[2 * FS + 2 * stride],
-                b3 = s[3 * FS + 2 * stride];
-    // characteristic differences y_n = L (U_n - U_i), n = i-2..i+3 (y_2 = 0)
-    float y[4][6];
-#pragma unroll
-    for (int n = 0; n < 6; n++) {
-        if (n == 2) continue;
-        float d0 = s[n * stride] - b0, d1 = s[FS + n * stride] - b1;
-        float d2 = s[2 * FS + n * stride] - b2, d3 = s[3 * FS + n * stride] - b3;
-        float c[4];
-        f32::project<DIR>(e, d0, d1, d2, d3, c);
-#pragma unroll
-        for (int k = 0; k < 4; k++) y[k][n] = c[k];
-    }
-    // both sides of each field in the two lanes (weno5_lanes); a field whose
-    // stencil is flat on both sides reconstructs its base values exactly, and
-    // uniform regions, where whole warps agree, skip the weights
-    f32::f2 W[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const unsigned any = (f32::bits(y[k][0]) | f32::bits(y[k][1]) | f32::bits(y[k][3]) |
-                              f32::bits(y[k][4]) | f32::bits(y[k][5])) << 1;
-        if (any == 0u) {
-            W[k] = f32::f2s(0.0f);
-        } else {
-            const float y3 = y[k][3];
-            W[k] = f32::weno5_lanes<WZ>(make_float2(y[k][0], y[k][5] - y3),
-                                        make_float2(y[k][1], y[k][4] - y3), make_float2(y3, -y3),
-                                        make_float2(y[k][4], y[k][1] - y3));
-        }
-    }
+}
+
+// Is either cell next to an interface near vacuum (p below pthr, 1e-3 of the
+// mean pressure)?
+EB2_HD bool near_vacuum(const float* pa, const float* pb, float pthr) {
+    return pa[f32::P_P * PS] < pthr || pb[f32::P_P * PS] < pthr;
+}
+
+// One interface.  s: stencil cell n = 0 of field 0 (fields FS apart, `stride`
+// along the sweep); pa/pb: primitive records of cells i and i+1 (fields PS
+// apart); ga/gb: the two cells in global memory.  VAC: an interface next to a
+// near-vacuum cell, whose characteristic projections take FP64 matrices
+// (vacuum_delta).
+template <bool VAC, int DIR, bool WZ, int FLUX>
+EB2_HD unsigned face_flux(const float* __restrict__ s, int stride, const float* __restrict__ pa,
+                          const float* __restrict__ pb, const double* __restrict__ u, size_t ga,
+                          size_t gb, size_t plane, const Gas& g, int positivity,
+                          float* __restrict__ out, int ostride) {
+    const float gm1 = (float)g.gm1, gamma = (float)g.gamma;
+    const float b3 = s[3 * FS + 2 * stride];
     f32::f2 dq[4];
-    f32::unproject2<DIR>(e, W, dq);
+    if constexpr (VAC) {
+        vacuum_delta<DIR, WZ>(u, ga, (long long)gb - (long long)ga, plane, g, dq);
+    } else {
+        const f32::Eig e = f32::roe_f32(pa, pb, PS, gm1);
+        const float b0 = s[2 * stride], b1 = s[FS + 2 * stride], b2 = s[2 * FS + 2 * stride];
+        // characteristic differences y_n = L (U_n - U_i), n = i-2..i+3 (y_2 = 0)
+        float y[4][6];
+#pragma unroll
+        for (int n = 0; n < 6; n++) {
+            if (n == 2) continue;
+            float d0 = s[n * stride] - b0, d1 = s[FS + n * stride] - b1;
+            float d2 = s[2 * FS + n * stride] - b2, d3 = s[3 * FS + n * stride] - b3;
+            float c[4];
+            f32::project<DIR>(e, d0, d1, d2, d3, c);
+#pragma unroll
+            for (int k = 0; k < 4; k++) y[k][n] = c[k];
+        }
+        // both sides of each field in the two lanes (weno5_lanes); a field whose
+        // stencil is flat on both sides reconstructs its base values exactly, and
+        // uniform regions, where whole warps agree, skip the weights
+        f32::f2 W[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const unsigned any = (f32::bits(y[k][0]) | f32::bits(y[k][1]) |
+                                  f32::bits(y[k][3]) | f32::bits(y[k][4]) |
+                                  f32::bits(y[k][5])) << 1;
+            if (any == 0u) {
+                W[k] = f32::f2s(0.0f);
+            } else {
+                const float y3 = y[k][3];
+                W[k] = f32::weno5_lanes<WZ>(make_float2(y[k][0], y[k][5] - y3),
+                                            make_float2(y[k][1], y[k][4] - y3),
+                                            make_float2(y3, -y3),
+                                            make_float2(y[k][4], y[k][1] - y3));
+            }
+        }
+        f32::unproject2<DIR>(e, W, dq);
+    }
     // minus side around cell i, plus side around cell i+1
     const float ra = pa[f32::P_RHO * PS], ua = pa[f32::P_U * PS], va = pa[f32::P_V * PS],
                 pas = pa[f32::P_P * PS];
@@ -124,6 +187,20 @@ EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
     out[2 * ostride] = DIR == 1 ? F[2] : F[1];
     out[3 * ostride] = F[3];
     return st;
+}
+
+// Both paths, chosen per interface (the CPU checks of the face arithmetic).
+template <int DIR, bool WZ, int FLUX>
+EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
+                               const float* __restrict__ pa, const float* __restrict__ pb,
+                               const double* __restrict__ u, size_t ga, size_t gb, size_t plane,
+                               float pthr, const Gas& g, int positivity, float* __restrict__ out,
+                               int ostride) {
+    if (near_vacuum(pa, pb, pthr))
+        return face_flux<true, DIR, WZ, FLUX>(s, stride, pa, pb, u, ga, gb, plane, g, positivity,
+                                              out, ostride);
+    return face_flux<false, DIR, WZ, FLUX>(s, stride, pa, pb, u, ga, gb, plane, g, positivity,
+                                           out, ostride);
 }
 
 // One tile (ti, tj) of one stage; shared by the single-solve and batched kernels.
@@ -177,32 +254,45 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     }
     __syncthreads();
 
-    // 2. interface fluxes
-    unsigned st = 0;
+    // 2. interface fluxes.  Interfaces next to a near-vacuum cell are marked
+    // in `vac` (bit = this thread's job number) and computed in a pass of
+    // their own with the FP64 eigenvector matrices.
+    unsigned st = 0, vac = 0;
     const int pos = a.num.positivity;
-    for (int job = threadIdx.x; job < NJX + NJY; job += NT) {
+    static_assert((NJX + NJY + NT - 1) / NT <= 32, "one vacuum bit per job of a thread");
+    auto face = [&](auto vacuum, int job) -> unsigned {
+        constexpr bool VAC = decltype(vacuum)::value;
         if (job < NJX) {
             int rr = job / TY, cc = job - rr * TY;
             int i = i0 - 1 + rr, j = j0 + cc;
-            if (i >= rows - GC || j >= cols - GC) continue;  // past the domain edge
+            if (i >= rows - GC || j >= cols - GC) return 0u;  // past the domain edge
             size_t ga = (size_t)i * cols + j;
             const float* pa = sP + rr * PY + (cc + 1);
-            st |= interface_flux<1, WZ, FLUX>(sU + rr * HY + (cc + 3), HY, pa, pa + PY, uin, ga,
-                                              ga + cols, plane, pthr, g, pos, sFx + rr * TY + cc,
-                                              XS);
-        } else {
-            int q = job - NJX;
-            int rr = q / (TY + 1), cc = q - rr * (TY + 1);
-            int i = i0 + rr, j = j0 - 1 + cc;
-            if (i >= rows - GC || j >= cols - GC) continue;
-            size_t ga = (size_t)i * cols + j;
-            const float* pa = sP + (rr + 1) * PY + cc;
-            st |= interface_flux<2, WZ, FLUX>(sU + (rr + 3) * HY + cc, 1, pa, pa + 1, uin, ga,
-                                              ga + 1, plane, pthr, g, pos,
-                                              sFy + rr * (TY + 1) + cc, YS);
+            if (!VAC && near_vacuum(pa, pa + PY, pthr)) return ~0u;
+            return face_flux<VAC, 1, WZ, FLUX>(sU + rr * HY + (cc + 3), HY, pa, pa + PY, uin,
+                                               ga, ga + cols, plane, g, pos,
+                                               sFx + rr * TY + cc, XS);
         }
+        int q = job - NJX;
+        int rr = q / (TY + 1), cc = q - rr * (TY + 1);
+        int i = i0 + rr, j = j0 - 1 + cc;
+        if (i >= rows - GC || j >= cols - GC) return 0u;
+        size_t ga = (size_t)i * cols + j;
+        const float* pa = sP + (rr + 1) * PY + cc;
+        if (!VAC && near_vacuum(pa, pa + 1, pthr)) return ~0u;
+        return face_flux<VAC, 2, WZ, FLUX>(sU + (rr + 3) * HY + cc, 1, pa, pa + 1, uin, ga,
+                                           ga + 1, plane, g, pos, sFy + rr * (TY + 1) + cc, YS);
+    };
+    for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++) {
+        const unsigned r = face(std::false_type{}, job);
+        if (r == ~0u) vac |= 1u << n;
+        else st |= r;
     }
-    __syncthreads();
+    if (__syncthreads_or(vac != 0u)) {
+        for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++)
+            if (vac >> n & 1u) st |= face(std::true_type{}, job);
+        __syncthreads();
+    }
 
     // 3. flux difference (widened to FP64), RK combination in FP64
     const double dt = ctrl->dt;

@@ -109,7 +109,10 @@ class Server:
     def active(self) -> int:
         return self.stats()["active"]
 
-    def run_trace(self, reqs: list[Request], arrival_s, keep_results: bool = False):
+    def run_trace(self, reqs: list[Request], arrival_s, keep_results=False):
+        """Replay a trace in real time.  keep_results: False, True (every
+        request's final state) or a collection of request indices whose final
+        states are kept (the others are dropped at retirement)."""
         n = len(reqs)
         arr = (_Req * n)(*[r.to_c() for r in reqs])
         t_arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
@@ -120,9 +123,11 @@ class Server:
         span = C.c_double()
         results = None
         res_ptrs = None
-        if keep_results:
-            results = [np.zeros((4, r.nx + 8, r.ny + 8)) for r in reqs]
-            res_ptrs = (_dp * n)(*[L.dptr(a) for a in results])
+        if keep_results is not False:
+            keep = set(range(n)) if keep_results is True else set(keep_results)
+            results = [np.zeros((4, r.nx + 8, r.ny + 8)) if i in keep else None
+                       for i, r in enumerate(reqs)]
+            res_ptrs = (_dp * n)(*[L.dptr(a) if a is not None else None for a in results])
         L.check(self._lib.eb2_server_run_trace(self._h, arr, L.dptr(t_arr), n, L.dptr(admit),
                                                L.dptr(finish), steps, status, res_ptrs,
                                                C.byref(span)))

@@ -30,15 +30,18 @@ unsigned mixed_face(const double* cells, double pthr, const Gas& g, int pos, dou
     static float sU[4 * mixstage::FS], sP[f32::NP * mixstage::PS];
     for (int n = 0; n < 6; n++)
         for (int k = 0; k < 4; k++) sU[k * mixstage::FS + n] = (float)cells[4 * n + k];
-    double u[8];
+    // the six cells in FP64 as the kernel's near-vacuum path reads them from
+    // the stage input: field planes of 6 values, cell i at index 2
+    double u[24];
+    for (int n = 0; n < 6; n++)
+        for (int k = 0; k < 4; k++) u[n + 6 * k] = cells[4 * n + k];
     for (int c = 0; c < 2; c++) {
         float qf[4];
         for (int k = 0; k < 4; k++) qf[k] = (float)cells[4 * (2 + c) + k];
         f32::cell_prims(cells + 4 * (2 + c), qf, g, sP + c, mixstage::PS);
-        for (int k = 0; k < 4; k++) u[c + 2 * k] = cells[4 * (2 + c) + k];
     }
     float Ff[4];
-    unsigned st = mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, sP, sP + 1, u, 0, 1, 2,
+    unsigned st = mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, sP, sP + 1, u, 2, 3, 6,
                                                           (float)pthr, g, pos, Ff, 1);
     for (int k = 0; k < 4; k++) F[k] = Ff[k];
     return st;

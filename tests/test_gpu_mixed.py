@@ -137,3 +137,34 @@ def test_mixed_near_vacuum_path(gpu):
     # pressure in the band to 1e-4 relative; density L1 as for the other runs
     assert np.max(np.abs(pb - pa)[band] / pa[band]) < 1e-4
     assert float(np.mean(np.abs(out["mixed"][0] - out["fp64"][0]))) < L1_TOL
+
+
+def test_mixed_near_vacuum_quadrant(gpu):
+    """A sharp near-vacuum case that the FP64 form survives: the four-quadrant
+    problem with the lower-left quadrant at p = 1e-5 (1.6e-5 of the mean
+    pressure), moving diagonally into the other three, 128^2 to t = 0.1.  The
+    shocks of the neighbouring quadrants run into near vacuum, where the mixed
+    form projects with the FP64 eigenvector matrices.  It stays finite and
+    positive, follows the FP64 form in density (L1 as for the other runs) and
+    in the pressure of the near-vacuum region."""
+    n = 128
+    q = [1.5, 0.0, 0.0, 1.5, 0.5323, 1.206, 0.0, 0.3, 0.138, 1.206, 1.206, 1.0e-5,
+         0.5323, 0.0, 1.206, 0.3]
+    out = {}
+    for name in ("fp64", "mixed"):
+        prec = gpu.lib.MIXED if name == "mixed" else gpu.lib.FP64
+        with gpu.Solver(n, n, precision=prec, recon=5, characteristic=True,
+                        weno_z=False) as s:
+            s.init_case(gpu.lib.CASE_FOUR_QUADRANT, q)
+            s.run(3, 2, 1 / n, 1 / n, 0.1)
+            assert s.status() == 0
+            out[name] = interior(s.con_to_pri())
+    a, b = out["fp64"], out["mixed"]
+    vac = a[3] < 1e-3 * a[3].mean()
+    assert vac.sum() > n * n // 10                     # the near-vacuum region is large
+    assert np.all(np.isfinite(b)) and b[0].min() > 0 and b[3].min() > 0
+    rel_p = np.abs(b[3] - a[3])[vac] / a[3][vac]
+    print(f"near-vacuum quadrant: density L1 {np.mean(np.abs(b[0] - a[0])):.3e}, "
+          f"pressure there max rel {rel_p.max():.3e}")
+    assert rel_p.max() < 1e-3
+    assert float(np.mean(np.abs(b[0] - a[0]))) < L1_TOL
