@@ -205,6 +205,18 @@ int eb2_rk_step(eb2_ctx *ctx, int order, int scheme, double dt, double dx, doubl
  * without host round trips.  At each output time the loop pauses and calls
  * on_output(user, time, step) (may be NULL), from which the caller may read
  * the state.  Returns the step count and the final time. */
+/* RK1_TimeAd_BS (include/time_advance.h:886-1025): one forward-Euler step of the
+ * backward-step flow on the context's state.  Block 1 (the channel above the
+ * step: all nx rows, int(0.8 ny) columns from column int(0.2 ny)) and block 2
+ * (the inlet section beside the step: int(0.2 nx) x int(0.2 ny) at the lower
+ * left) are advanced with their own ghost layers, filled by the rules of
+ * BC_BackwardStep_2D (include/Boundary_Condition.h:696-850); the rest of the
+ * lower strip is the step and keeps its values.  The context's
+ * reconstruction, gas and gravity source apply; the step runs in the FP64
+ * form whatever the context's precision (the reference's bits).  Returns
+ * EB2_ENONPHYS if a non-physical state was met. */
+int eb2_rk1_backward_step(eb2_ctx *ctx, int scheme, double dt, double dx, double dy);
+
 typedef void (*eb2_output_fn)(void *user, double time, long long step);
 int eb2_run(eb2_ctx *ctx, int order, int scheme, double dx, double dy, double t0,
             double tmax, int n_out, eb2_output_fn on_output, void *user, long long *steps,

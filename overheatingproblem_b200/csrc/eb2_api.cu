@@ -745,6 +745,80 @@ int eb2_rk_step(eb2_ctx* c, int order, int scheme, double dt, double dx, double 
     return EB2_OK;
 }
 
+// RK1_TimeAd_BS (include/time_advance.h:886-1025): one forward-Euler step of
+// the backward-step flow on two blocks, every part on the GPU.  Block 1 is
+// the channel above the step (all nx rows, int(0.8 ny) columns starting
+// int(0.2 ny) in), block 2 the inlet section beside the step (int(0.2 nx) x
+// int(0.2 ny) at the lower left); the rest of the lower strip is the step and
+// is not advanced.  Each block is gathered out of the state into a stage
+// buffer of its own, its ghost layers are filled by BC_BackwardStep_2D's rules,
+// the fused FP64 stage (flux reconstruction, flux difference, gravity source,
+// Euler update) runs on it, and the block interiors are scattered back.  The
+// FP64 stage runs whatever the context's precision: the reference's bits.
+int eb2_rk1_backward_step(eb2_ctx* c, int scheme, double dt, double dx, double dy) {
+    if (int r = check(c)) return r;
+    const int G = GC;
+    const int LNX = c->grid.nx, LNY = c->grid.ny;
+    const int off = (int)(LNY * 0.2);
+    Grid g1 = c->grid, g2 = c->grid;
+    g1.rows = LNX + 2 * G;
+    g1.cols = (int)(LNY * 0.8 + 2 * G);
+    g2.rows = (int)(LNX * 0.2 + 2 * G);
+    g2.cols = (int)(LNY * 0.2 + 2 * G);
+    if (g2.rows < 2 * G + 1 || g2.cols < 2 * G + 1 || g1.cols < 2 * G + 1)
+        return fail(EB2_EARG, "RK1_TimeAd_BS: grid %d x %d too small for the two blocks", LNX,
+                    LNY);
+    g1.nx = g1.rows - 2 * G;
+    g1.ny = g1.cols - 2 * G;
+    g2.nx = g2.rows - 2 * G;
+    g2.ny = g2.cols - 2 * G;
+    int flux;
+    if (int r = map_scheme(scheme, &flux)) return r;
+    c->num.flux = flux;
+    set_spacing(c, dx, dy);
+    g1.dx = g2.dx = c->grid.dx;
+    g1.dy = g2.dy = c->grid.dy;
+    g1.inv_dx = g2.inv_dx = c->grid.inv_dx;
+    g1.inv_dy = g2.inv_dy = c->grid.inv_dy;
+    if (int r = ensure_tmp(c, 2)) return r;
+    // block 1 in u1 -> u2, block 2 in tmp[0] -> tmp[1] (each fits a state array)
+    double *b1 = c->u1, *o1 = c->u2, *b2 = c->tmp[0], *o2 = c->tmp[1];
+    Boundary in{};
+    const double gm = c->gas.gamma;
+    in.inflow[0] = 1.4;
+    in.inflow[1] = 1.4 * 3.0;
+    in.inflow[2] = 0.0;
+    in.inflow[3] = 1.0 / (gm - 1) + 0.5 * 1.4 * 3 * 3;
+    unsigned before = 0, after = 0;
+    if (int r = read_status(c, &before)) return r;
+    k_set_step<<<1, 1, 0, c->stream>>>(c->ctrl, 0.0, dt);
+    CK(cudaGetLastError());
+    CK(launch_bs_gather(c->u, c->grid, b1, g1, b2, g2, off, c->stream));
+    CK(launch_bs_boundary(b1, g1, b2, g2, in, c->stream));
+    double* ins[2] = {b1, b2};
+    double* outs[2] = {o1, o2};
+    const Grid* gs[2] = {&g1, &g2};
+    for (int q = 0; q < 2; q++) {
+        StageArgs a;
+        a.uin = ins[q];
+        a.un = ins[q];
+        a.uout = outs[q];
+        a.grid = *gs[q];
+        a.gas = c->gas;
+        a.num = c->num;
+        a.combine = COMB_EULER;
+        a.ctrl = c->ctrl;
+        a.partials = nullptr;
+        CK(launch_stage_fp64(a, c->stream));
+    }
+    CK(launch_bs_scatter(c->u, c->grid, o1, g1, o2, g2, off, c->stream));
+    c->launches += 6;
+    if (int r = read_status(c, &after)) return r;
+    if ((after & ~before) & (ST_NONPHYSICAL | ST_NAN_STATE))
+        return fail(EB2_ENONPHYS, "non-physical state met (status 0x%x)", after);
+    return EB2_OK;
+}
+
 }  // extern "C"
 
 namespace {

@@ -486,3 +486,156 @@ cudaError_t launch_space_item(const double* f, const double* gflux, const double
 }
 
 }  // namespace eb2
+
+// ---------------------------------------------------------------------------
+// The backward-step flow's two-block step (RK1_TimeAd_BS,
+// include/time_advance.h:886-1025): block 1 is the channel above the step,
+// block 2 the inlet section beside it; each is a [4][rows][cols] array of its
+// own with 4 ghost layers.
+// ---------------------------------------------------------------------------
+namespace eb2 {
+namespace {
+
+// Interiors of both blocks from U (block 1 starts `off` columns in), the
+// rest of each block zero, as the reference starts its block arrays.
+__global__ void k_bs_gather(const double* __restrict__ u, Grid g, double* __restrict__ b1,
+                            Grid g1, double* __restrict__ b2, Grid g2, int off) {
+    const long long n1 = 4LL * g1.rows * g1.cols, n = n1 + 4LL * g2.rows * g2.cols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const bool first = e < n1;
+        const Grid& b = first ? g1 : g2;
+        const long long r = first ? e : e - n1;
+        const long long plane = (long long)b.rows * b.cols;
+        const int k = (int)(r / plane);
+        const int i = (int)((r - k * plane) / b.cols), j = (int)(r - k * plane - (long long)i * b.cols);
+        double v = 0.0;
+        if (i >= GC && i < b.rows - GC && j >= GC && j < b.cols - GC)
+            v = u[at(k, i, j + (first ? off : 0), g.rows, g.cols)];
+        (first ? b1 : b2)[r] = v;
+    }
+}
+
+// Ghost layers of both blocks by the rules of BC_BackwardStep_2D
+// (include/Boundary_Condition.h:696-850): inflow on both blocks' left sides,
+// zero-gradient outflow on block 1's right, reflecting walls (the normal
+// momentum mirrored with its sign flipped) below and above block 1, below
+// block 2 and on block 2's right (the step face), and where the blocks meet
+// block 2's top ghosts from block 1's first interior columns and block 1's
+// bottom ghosts from block 2's last ones (that exchange is the last write of
+// the reference, so it wins over the wall rule on block 1's bottom).  Every
+// ghost value is a copy of an interior value or the inflow state, so one
+// thread per ghost element gives the reference's values in any order.
+// Corners stay as they are: no stencil reads them.
+__global__ void k_bs_boundary(double* __restrict__ b1, Grid g1, double* __restrict__ b2,
+                              Grid g2, Boundary inflow) {
+    // per block and field: 4 sides x GC layers x (rows or cols) candidates
+    const int per1 = 2 * GC * (g1.rows + g1.cols), per2 = 2 * GC * (g2.rows + g2.cols);
+    const long long n = 4LL * (per1 + per2);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const bool first = e < 4LL * per1;
+        const long long r = first ? e : e - 4LL * per1;
+        const Grid& b = first ? g1 : g2;
+        double* x = first ? b1 : b2;
+        const int per = first ? per1 : per2;
+        const int k = (int)(r / per);
+        int q = (int)(r - (long long)k * per);
+        const int R = b.rows, C = b.cols;
+        // sides: 0 left (i < GC), 1 right (i >= R-GC) over interior j;
+        //        2 bottom (j < GC), 3 top (j >= C-GC) over interior i
+        int side, m, t;
+        if (q < 2 * GC * C) {
+            side = q / (GC * C);
+            q -= side * GC * C;
+            m = q / C;
+            t = q - m * C;
+            if (t < GC || t >= C - GC) continue;
+        } else {
+            q -= 2 * GC * C;
+            side = 2 + q / (GC * R);
+            q -= (side - 2) * GC * R;
+            m = q / R;
+            t = q - m * R;
+            if (t < GC || t >= R - GC) continue;
+        }
+        double v;
+        int i, j;
+        if (side == 0) {            // inflow
+            i = m;
+            j = t;
+            v = inflow.inflow[k];
+        } else if (side == 1) {     // block 1: outflow; block 2: the step face, a wall
+            i = R - GC + m;
+            j = t;
+            if (first) {
+                v = x[at(k, R - GC - 1, j, R, C)];
+            } else {
+                v = x[at(k, R - GC - 1 - m, j, R, C)];
+                if (k == 1) v = -v;
+            }
+        } else if (side == 2) {     // bottom: wall, or block 2's last columns
+            i = t;
+            j = m;
+            if (first && i < g2.rows - GC) {
+                v = b2[at(k, i, g2.cols - 2 * GC + m, g2.rows, g2.cols)];
+            } else {
+                v = x[at(k, i, 2 * GC - 1 - m, R, C)];
+                if (k == 2) v = -v;
+            }
+        } else {                    // top: block 1 wall; block 2 from block 1
+            i = t;
+            j = C - GC + m;
+            if (first) {
+                v = x[at(k, i, C - GC - 1 - m, R, C)];
+                if (k == 2) v = -v;
+            } else {
+                v = b1[at(k, i, GC + m, g1.rows, g1.cols)];
+            }
+        }
+        x[at(k, i, j, R, C)] = v;
+    }
+}
+
+// Interiors of both blocks back into U.
+__global__ void k_bs_scatter(double* __restrict__ u, Grid g, const double* __restrict__ b1,
+                             Grid g1, const double* __restrict__ b2, Grid g2, int off) {
+    const long long n1 = 4LL * g1.nx * g1.ny, n = n1 + 4LL * g2.nx * g2.ny;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const bool first = e < n1;
+        const Grid& b = first ? g1 : g2;
+        const long long r = first ? e : e - n1;
+        const long long plane = (long long)b.nx * b.ny;
+        const int k = (int)(r / plane);
+        const int i = GC + (int)((r - k * plane) / b.ny);
+        const int j = GC + (int)(r - k * plane - (long long)(i - GC) * b.ny);
+        u[at(k, i, j + (first ? off : 0), g.rows, g.cols)] =
+            (first ? b1 : b2)[at(k, i, j, b.rows, b.cols)];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_bs_gather(const double* u, const Grid& g, double* b1, const Grid& g1,
+                             double* b2, const Grid& g2, int off, cudaStream_t s) {
+    const long long n = 4LL * g1.rows * g1.cols + 4LL * g2.rows * g2.cols;
+    k_bs_gather<<<blocks_for(n), NT, 0, s>>>(u, g, b1, g1, b2, g2, off);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bs_boundary(double* b1, const Grid& g1, double* b2, const Grid& g2,
+                               const Boundary& inflow, cudaStream_t s) {
+    const long long n = 4LL * 2 * GC * (g1.rows + g1.cols + g2.rows + g2.cols);
+    k_bs_boundary<<<blocks_for(n), NT, 0, s>>>(b1, g1, b2, g2, inflow);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bs_scatter(double* u, const Grid& g, const double* b1, const Grid& g1,
+                              const double* b2, const Grid& g2, int off, cudaStream_t s) {
+    const long long n = 4LL * g1.nx * g1.ny + 4LL * g2.nx * g2.ny;
+    k_bs_scatter<<<blocks_for(n), NT, 0, s>>>(u, g, b1, g1, b2, g2, off);
+    return cudaGetLastError();
+}
+
+}  // namespace eb2

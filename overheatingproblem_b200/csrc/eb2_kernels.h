@@ -60,6 +60,16 @@ cudaError_t launch_finalize(Ctrl* ctrl, const double* partials, int nblocks, int
 cudaError_t launch_copy_interior(double* dst, const double* src, const Grid& g,
                                  cudaStream_t s);
 
+// The backward-step flow's two-block step (RK1_TimeAd_BS): block interiors
+// out of U (block 1 starting `off` columns in), the ghost layers of both
+// blocks (Boundary::inflow holds the inflow state), block interiors back.
+cudaError_t launch_bs_gather(const double* u, const Grid& g, double* b1, const Grid& g1,
+                             double* b2, const Grid& g2, int off, cudaStream_t s);
+cudaError_t launch_bs_boundary(double* b1, const Grid& g1, double* b2, const Grid& g2,
+                               const Boundary& inflow, cudaStream_t s);
+cudaError_t launch_bs_scatter(double* u, const Grid& g, const double* b1, const Grid& g1,
+                              const double* b2, const Grid& g2, int off, cudaStream_t s);
+
 // Granular reference entry points (one thread per interface or cell).
 cudaError_t launch_con_to_pri(const double* u, double* pri, const Grid& g, const Gas& gas,
                               cudaStream_t s);

@@ -346,166 +346,18 @@ int rpf_space_discrete(int rows, int cols, double dx, double dy, const double *f
  * the channel above the step (the whole length, the upper part of the height,
  * int(0.8 ny) cells), block 2 the inlet section beside the step (int(0.2 nx)
  * by int(0.2 ny) cells at the lower left).  The rest of the lower strip is
- * the step and is not advanced.  Each call starts both blocks from zero,
- * copies their interiors out of U, forms the gravity source when Source is
- * set, fills the ghost layers by the rules of BC_BackwardStep_2D
- * (include/Boundary_Condition.h:696-850: Mach-3 inflow on the left,
- * zero-gradient outflow on block 1's right, reflecting walls, block 2's right
- * face a wall, and the two blocks exchanging four layers where they meet),
- * then runs the flux reconstruction and the flux difference of each block on
- * the GPU and adds dt times it on the host, and copies the interiors back.
- * The host part is plain C with no contraction, so the result has the
- * reference's bits. */
-
-enum { GC_ROWS = 4 };   /* ghost layers on each side */
-
-static double *g_bs_buf;
-static size_t g_bs_len;
-
-static int bs_arrays(size_t n1, size_t n2, double **a1, double **a2) {
-    size_t need = 5 * (n1 + n2);
-    if (need > g_bs_len) {
-        if (g_bs_buf) {
-            /* the blocks' device copies are bound to the old host addresses */
-            for (int k = 0; k < MAX_BINDINGS; k++)
-                if (g_bind[k].ctx && g_bind[k].host >= g_bs_buf &&
-                    g_bind[k].host < g_bs_buf + g_bs_len)
-                    drop(&g_bind[k]);
-            free(g_bs_buf);
-        }
-        g_bs_buf = (double *)malloc(need * sizeof(double));
-        g_bs_len = g_bs_buf ? need : 0;
-        if (!g_bs_buf) return fail(EB2_ENOMEM, "host allocation of the step blocks failed");
-    }
-    memset(g_bs_buf, 0, need * sizeof(double));
-    *a1 = g_bs_buf;
-    *a2 = g_bs_buf + 5 * n1;
-    return EB2_OK;
-}
-
-/* Source_Gravity (include/scheme.h:3723-3750) over a block's interior. */
-static void bs_source(int rows, int cols, const double *u, double *s, double gravity) {
-    const size_t pl = (size_t)rows * cols;
-    for (int i = GC_ROWS; i <= rows - GC_ROWS - 1; i++)
-        for (int j = GC_ROWS; j <= cols - GC_ROWS - 1; j++) {
-            const size_t o = (size_t)i * cols + j;
-            const double rho = u[o], v = u[2 * pl + o] / rho;
-            s[o] = 0.0;
-            s[pl + o] = 0.0;
-            s[2 * pl + o] = rho * gravity;
-            s[3 * pl + o] = rho * gravity * v;
-        }
-}
-
-/* Ghost layers of both blocks, in the order of BC_BackwardStep_2D. */
-static void bs_boundary(int r1, int c1, double *x, int r2, int c2, double *y, double gamma) {
-    const int G = GC_ROWS;
-    const size_t p1 = (size_t)r1 * c1, p2 = (size_t)r2 * c2;
-#define X(k, i, j) x[(k) * p1 + (size_t)(i) * c1 + (j)]
-#define Y(k, i, j) y[(k) * p2 + (size_t)(i) * c2 + (j)]
-    const double inflow[4] = {1.4, 1.4 * 3.0, 0.0, 1.0 / (gamma - 1) + 0.5 * 1.4 * 3 * 3};
-    /* block 1: inflow on the left */
-    for (int j = G; j < c1 - G; j++)
-        for (int k = 0; k < 4; k++)
-            for (int m = 1; m <= G; m++) X(k, G - m, j) = inflow[k];
-    /* block 1: zero-gradient outflow on the right */
-    for (int k = 0; k < 4; k++)
-        for (int j = G; j < c1 - G; j++)
-            for (int m = 0; m < G; m++) X(k, r1 - G + m, j) = X(k, r1 - G - 1, j);
-    /* block 1: walls below and above (y momentum mirrored with its sign flipped) */
-    for (int k = 0; k < 4; k++)
-        for (int i = G; i < r1 - G; i++)
-            for (int m = 1; m <= G; m++)
-                X(k, i, G - m) = k == 2 ? -X(k, i, G + m - 1) : X(k, i, G + m - 1);
-    for (int k = 0; k < 4; k++)
-        for (int i = G; i < r1 - G; i++)
-            for (int m = 0; m < G; m++)
-                X(k, i, c1 - G + m) = k == 2 ? -X(k, i, c1 - G - 1 - m) : X(k, i, c1 - G - 1 - m);
-    /* block 2: inflow on the left */
-    for (int j = G; j < c2 - G; j++)
-        for (int k = 0; k < 4; k++)
-            for (int m = 1; m <= G; m++) Y(k, G - m, j) = inflow[k];
-    /* block 2: the step face on the right, a wall (x momentum flipped) */
-    for (int k = 0; k < 4; k++)
-        for (int j = G; j < c2 - G; j++)
-            for (int m = 0; m < G; m++)
-                Y(k, r2 - G + m, j) = k == 1 ? -Y(k, r2 - G - 1 - m, j) : Y(k, r2 - G - 1 - m, j);
-    /* block 2: wall below */
-    for (int k = 0; k < 4; k++)
-        for (int i = G; i < r2 - G; i++)
-            for (int m = 1; m <= G; m++)
-                Y(k, i, G - m) = k == 2 ? -Y(k, i, G + m - 1) : Y(k, i, G + m - 1);
-    /* where the blocks meet: block 2's top ghosts from block 1's first rows,
-     * block 1's bottom ghosts from block 2's last rows */
-    for (int k = 0; k < 4; k++)
-        for (int i = G; i < r2 - G; i++)
-            for (int m = 0; m < G; m++) {
-                Y(k, i, c2 - G + m) = X(k, i, G + m);
-                X(k, i, m) = Y(k, i, c2 - 2 * G + m);
-            }
-#undef X
-#undef Y
-}
-
-/* Flux reconstruction and flux difference of one block on the GPU, then the
- * forward-Euler update of its interior on the host. */
-static int bs_block(int scheme, int rows, int cols, double *arr, double dt, double dx, double dy,
-                    const rpf_globals *g) {
-    const size_t n = (size_t)4 * rows * cols;
-    double *u = arr, *f = arr + n, *gf = arr + 2 * n, *s = arr + 3 * n, *si = arr + 4 * n;
-    binding *b;
-    TRY(bind(u, rows, cols, &b));
-    TRY(configure(b, g, 0));
-    b->state = HOST_NEWER;
-    TRY(push(b));
-    LIB(eb2_flux_reconstruction(b->ctx, scheme, dx, dy, f, gf), "Flux_Reconstruction_RP");
-    LIB(eb2_space_discrete(b->ctx, dx, dy, f, gf, s, si), "Space_Discrete_Item");
-    const size_t pl = (size_t)rows * cols;
-    for (int i = GC_ROWS; i <= rows - GC_ROWS - 1; i++)
-        for (int j = GC_ROWS; j <= cols - GC_ROWS - 1; j++)
-            for (int k = 0; k < 4; k++) {
-                const size_t o = k * pl + (size_t)i * cols + j;
-                u[o] = u[o] + dt * si[o];
-            }
-    return EB2_OK;
-}
-
+ * the step and is not advanced.  The whole step runs on the GPU
+ * (eb2_rk1_backward_step): block gather, the ghost layers of
+ * BC_BackwardStep_2D, the gravity source, flux reconstruction, flux
+ * difference and Euler update of each block, and the scatter back into U. */
 int rpf_rk1_bs(int scheme, int rows, int cols, double *U, double dt, double dx, double dy,
                const rpf_globals *g) {
-    const int G = GC_ROWS;
-    const int LNX = rows - 2 * G, LNY = cols - 2 * G;
-    const int B2_LNY = (int)(LNY * 0.2);
-    const int r1 = LNX + 2 * G, c1 = (int)(LNY * 0.8 + 2 * G);
-    const int r2 = (int)(LNX * 0.2 + 2 * G), c2 = (int)(LNY * 0.2 + 2 * G);
-    if (r2 < 2 * G + 1 || c2 < 2 * G + 1 || c1 < 2 * G + 1)
-        return fail(EB2_EARG, "RK1_TimeAd_BS: grid %d x %d too small for the two blocks",
-                    LNX, LNY);
-    TRY(rpf_sync_host(U));
-    double *a1, *a2;
-    TRY(bs_arrays((size_t)4 * r1 * c1, (size_t)4 * r2 * c2, &a1, &a2));
-    const size_t pu = (size_t)rows * cols, p1 = (size_t)r1 * c1, p2 = (size_t)r2 * c2;
-    for (int k = 0; k < 4; k++) {
-        for (int i = G; i < r1 - G; i++)
-            for (int j = G; j < c1 - G; j++)
-                a1[k * p1 + (size_t)i * c1 + j] = U[k * pu + (size_t)i * cols + j + B2_LNY];
-        for (int i = G; i < r2 - G; i++)
-            for (int j = G; j < c2 - G; j++)
-                a2[k * p2 + (size_t)i * c2 + j] = U[k * pu + (size_t)i * cols + j];
-    }
-    if (g->source) {
-        bs_source(r1, c1, a1, a1 + 12 * p1, g->gravity);
-        bs_source(r2, c2, a2, a2 + 12 * p2, g->gravity);
-    }
-    bs_boundary(r1, c1, a1, r2, c2, a2, g->gamma);
-    TRY(bs_block(scheme, r1, c1, a1, dt, dx, dy, g));
-    TRY(bs_block(scheme, r2, c2, a2, dt, dx, dy, g));
-    for (int k = 0; k < 4; k++) {
-        for (int i = G; i < r1 - G; i++)
-            for (int j = G; j < c1 - G; j++)
-                U[k * pu + (size_t)i * cols + j + B2_LNY] = a1[k * p1 + (size_t)i * c1 + j];
-        for (int i = G; i < r2 - G; i++)
-            for (int j = G; j < c2 - G; j++)
-                U[k * pu + (size_t)i * cols + j] = a2[k * p2 + (size_t)i * c2 + j];
-    }
-    return rpf_host_modified(U);
+    binding *b;
+    TRY(bind(U, rows, cols, &b));
+    TRY(configure(b, g, 0));
+    TRY(push(b));
+    int rc = eb2_rk1_backward_step(b->ctx, scheme, dt, dx, dy);
+    if (rc && rc != EB2_ENONPHYS) return lib_fail(rc, "RK1_TimeAd_BS");
+    TRY(device_wrote(b));
+    return note_status(rc);
 }

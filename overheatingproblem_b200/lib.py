@@ -121,6 +121,7 @@ SIGNATURES = {
     "eb2_server_run_trace": (C.c_int, [_vp, C.POINTER(Request), _dp, C.c_int, _dp, _dp,
                                        C.POINTER(C.c_longlong), C.POINTER(C.c_uint),
                                        C.POINTER(_dp), _dp]),
+    "eb2_rk1_backward_step": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double]),
     "eb2_rk_step_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(NoallocConfig), C.c_int,
                                       C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                       _vp]),
