@@ -27,6 +27,7 @@ struct SlotDesc {
     int tiles_x;          // tiles along y
     int ntiles;
     int ncells;
+    int bc_blocks;        // ghost-fill blocks of this slot (its entries in the bc work list)
 };
 
 // Stage buffers of SSP-RK3 (the server runs third-order steps only).
@@ -49,16 +50,22 @@ __device__ __forceinline__ StageArgs slot_args(const SlotDesc& s, int stage) {
     return a;
 }
 
-// Host-side launch interface (eb2_batch_fp64.cu / eb2_batch_mixed.cu).
+// Host-side launch interface (eb2_batch_fp64.cu / eb2_batch_mixed.cu).  The
+// three work lists are rewritten on admission and retirement only; the
+// kernels read their lengths from device memory, so that a captured launch
+// stays valid while its grid covers the list (grids are sized to powers of two).
 struct BatchLaunch {
     const SlotDesc* slots;   // device array of nslots descriptors
     int nslots;
-    const int2* work;        // device work list: (slot, tile)
-    const int* nwork;        // device: number of work items
-    int grid;                // persistent CTAs of the stage kernels
-    int bc_blocks;           // ghost-fill blocks per slot (sized for the largest slot)
-    int slot_range;          // slots 0 .. slot_range-1 hold every active one (the
-                             // ghost-fill and end-of-step grids cover only those)
+    const int2* work;        // device work list of the stage kernels: (slot, tile)
+    const int* nwork;        // device: its length
+    int grid;                // CTAs of the stage kernels
+    const int2* bc_work;     // device work list of the ghost fill: (slot, block of the slot)
+    const int* nbc;          // device: its length
+    int bc_grid;             // blocks of the ghost fill (>= *nbc)
+    const int* active;       // device list of the active slots (end-of-step reduction)
+    const int* nactive;      // device: its length
+    int active_grid;         // blocks of the end-of-step reduction (>= *nactive)
     int each = 0;            // 1: one CTA per work item (grid >= every work-list
                              // length it is used with), 0: persistent CTAs that loop
 };

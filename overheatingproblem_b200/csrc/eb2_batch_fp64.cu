@@ -90,34 +90,37 @@ cudaError_t launch_stage_batch_fp64(const BatchLaunch& b, const Numerics& num, i
                       : by_flux<5, true, false>(b, num.flux, stage, s);
 }
 
-// Boundary fill of stage `stage`'s input for every active slot: block row y
-// serves slot y.
-__global__ void k_bc_batch(const SlotDesc* __restrict__ slots, int stage) {
-    const SlotDesc& sd = slots[blockIdx.y];
+// Boundary fill of stage `stage`'s input for every active slot: each block
+// of the bc work list fills its share of one slot's ghost layers.
+__global__ void k_bc_batch(const SlotDesc* __restrict__ slots, const int2* __restrict__ work,
+                           const int* __restrict__ nwork, int stage) {
+    if ((int)blockIdx.x >= *nwork) return;
+    const int2 it = work[blockIdx.x];
+    const SlotDesc& sd = slots[it.x];
     if (!sd.ctrl || !sd.ctrl->active) return;
     double* u = stage == 0 ? sd.u : (stage == 1 ? sd.u1 : sd.u2);
-    bc_fill(u, sd.grid, sd.bnd, sd.ctrl->t, blockIdx.x * (long long)blockDim.x + threadIdx.x,
-            (long long)gridDim.x * blockDim.x);
+    bc_fill(u, sd.grid, sd.bnd, sd.ctrl->t, it.y * (long long)blockDim.x + threadIdx.x,
+            (long long)sd.bc_blocks * blockDim.x);
 }
 
 cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s) {
-    dim3 grid(b.bc_blocks > 0 ? b.bc_blocks : 8, b.slot_range > 0 ? b.slot_range : b.nslots);
-    k_bc_batch<<<grid, 256, 0, s>>>(b.slots, stage);
+    k_bc_batch<<<b.bc_grid, 256, 0, s>>>(b.slots, b.bc_work, b.nbc, stage);
     return cudaGetLastError();
 }
 
 // End of a step for every active slot: one block per slot.
-__global__ void k_finalize_batch(const SlotDesc* __restrict__ slots) {
+__global__ void k_finalize_batch(const SlotDesc* __restrict__ slots, const int* __restrict__ act,
+                                 const int* __restrict__ nact) {
     __shared__ double red[96];
-    const SlotDesc& sd = slots[blockIdx.x];
+    if ((int)blockIdx.x >= *nact) return;
+    const SlotDesc& sd = slots[act[blockIdx.x]];
     if (!sd.ctrl) return;
     finalize_body(sd.ctrl, sd.partials, sd.ntiles, sd.ncells, 2, red);
 }
 
 cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s) {
-    k_finalize_batch<<<b.slot_range > 0 ? b.slot_range : b.nslots, 256, 0, s>>>(b.slots);
+    k_finalize_batch<<<b.active_grid, 256, 0, s>>>(b.slots, b.active, b.nactive);
     return cudaGetLastError();
 }
-
 
 }  // namespace eb2

@@ -99,13 +99,20 @@ struct eb2_server {
     int* h_nwork = nullptr;       // pinned
     int work_cap = 0;
     int nwork = 0;
+    int2* d_bcwork = nullptr;     // ghost-fill work list: (slot, block of the slot)
+    int2* h_bcwork = nullptr;     // pinned
+    int* d_counts = nullptr;      // device: ghost-fill and active-slot list lengths
+    int* h_counts = nullptr;      // pinned
+    int* d_active = nullptr;      // active slot indices (end-of-step reduction)
+    int* h_active = nullptr;      // pinned
+    int bc_cap = 0;
     bool dirty = true;
     long long next_id = 0;
     int sms = 148;
     std::map<int, cudaGraphExec_t> graphs;   // launch key (grid_key) -> graph
     std::map<int, int> tuned;                // shape class -> launch key
-    int bc_blocks = 8;                       // ghost-fill blocks per slot
-    int slot_range = 1;                      // slots the per-slot kernels cover
+    int bc_grid = 8;                         // blocks of the ghost-fill launches
+    int active_grid = 8;                     // blocks of the end-of-step launches
     long long graph_launches = 0;
 };
 
@@ -131,7 +138,9 @@ int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
         *out = it->second;
         return EB2_OK;
     }
-    BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0, s->bc_blocks, s->slot_range};
+    BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0,
+                  s->d_bcwork, s->d_counts, s->bc_grid,
+                  s->d_active, s->d_counts + 1, s->active_grid};
     CKS(stage_batch(s, b, 0));  // kernel attributes, outside the capture
     b.grid = key / 2;
     b.each = key % 2;
@@ -176,21 +185,41 @@ int rebuild(eb2_server* s) {
         s->work_cap = cap;
         destroy_graphs(s);  // graphs hold the old work-list address
     }
-    // one ghost-fill thread per ghost column element of the largest active slot
-    // (32 (nx + ny) of them), as the single-solve fill launches
-    long long ghosts = 0;
-    int top = 0;
+    // ghost-fill blocks: each active slot takes enough 256-thread blocks for its
+    // 32 (nx + ny) ghost values (at most 256; the blocks loop beyond that)
+    int nbc = 0, nact = 0;
     for (int q = 0; q < s->nslots; q++)
         if (s->slots[q].used && !s->slots[q].done) {
-            ghosts = std::max(ghosts, 32LL * (s->h_desc[q].grid.nx + s->h_desc[q].grid.ny));
-            top = q + 1;
+            const Grid& g = s->h_desc[q].grid;
+            s->h_desc[q].bc_blocks =
+                (int)std::min<long long>((32LL * (g.nx + g.ny) + 255) / 256, 256);
+            nbc += s->h_desc[q].bc_blocks;
+            nact++;
         }
-    const int bc_blocks = (int)std::min<long long>(std::max<long long>((ghosts + 255) / 256, 8), 1024);
-    const int slot_range = std::max(top, 1);
-    if (bc_blocks != s->bc_blocks || slot_range != s->slot_range) {
-        s->bc_blocks = bc_blocks;
-        s->slot_range = slot_range;
-        destroy_graphs(s);  // graphs hold the per-slot grids
+    if (nbc > s->bc_cap) {
+        int cap = std::max(nbc, 2 * s->bc_cap);
+        if (s->d_bcwork) CKS(cudaFreeAsync(s->d_bcwork, s->stream));
+        if (s->h_bcwork) {
+            CKS(cudaStreamSynchronize(s->stream));
+            cudaFreeHost(s->h_bcwork);
+        }
+        CKS(cudaMallocAsync(&s->d_bcwork, (size_t)cap * sizeof(int2), s->stream));
+        CKS(cudaMallocHost(&s->h_bcwork, (size_t)cap * sizeof(int2)));
+        s->bc_cap = cap;
+        destroy_graphs(s);  // graphs hold the old list address
+    }
+    // launch grids: powers of two covering the lists, so that graphs are only
+    // captured again when a list outgrows its grid
+    auto pow2 = [](int n) {
+        int g = 8;
+        while (g < n) g *= 2;
+        return g;
+    };
+    const int bc_grid = pow2(nbc), active_grid = pow2(nact);
+    if (bc_grid != s->bc_grid || active_grid != s->active_grid) {
+        s->bc_grid = bc_grid;
+        s->active_grid = active_grid;
+        destroy_graphs(s);  // graphs hold the launch grids
     }
     CKS(cudaStreamSynchronize(s->stream));  // the pinned staging arrays are reused
     int w = 0;
@@ -200,9 +229,23 @@ int rebuild(eb2_server* s) {
     }
     *s->h_nwork = w;
     s->nwork = w;
+    int nb = 0, na = 0;
+    for (int q = 0; q < s->nslots; q++) {
+        if (!s->slots[q].used || s->slots[q].done) continue;
+        for (int k = 0; k < s->h_desc[q].bc_blocks; k++) s->h_bcwork[nb++] = make_int2(q, k);
+        s->h_active[na++] = q;
+    }
+    s->h_counts[0] = nb;
+    s->h_counts[1] = na;
     if (w) CKS(cudaMemcpyAsync(s->d_work, s->h_work, (size_t)w * sizeof(int2),
                                cudaMemcpyHostToDevice, s->stream));
     CKS(cudaMemcpyAsync(s->d_nwork, s->h_nwork, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    if (nb) CKS(cudaMemcpyAsync(s->d_bcwork, s->h_bcwork, (size_t)nb * sizeof(int2),
+                                cudaMemcpyHostToDevice, s->stream));
+    if (na) CKS(cudaMemcpyAsync(s->d_active, s->h_active, (size_t)na * sizeof(int),
+                                cudaMemcpyHostToDevice, s->stream));
+    CKS(cudaMemcpyAsync(s->d_counts, s->h_counts, 2 * sizeof(int), cudaMemcpyHostToDevice,
+                        s->stream));
     CKS(cudaMemcpyAsync(s->d_desc, s->h_desc, (size_t)s->nslots * sizeof(SlotDesc),
                         cudaMemcpyHostToDevice, s->stream));
     s->dirty = false;
@@ -344,7 +387,11 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
         cudaMallocHost(&s->h_desc, (size_t)max_slots * sizeof(SlotDesc)) ||
         cudaMalloc(&s->d_ctrl, (size_t)max_slots * sizeof(Ctrl)) ||
         cudaMallocHost(&s->h_ctrl, (size_t)max_slots * sizeof(Ctrl)) ||
-        cudaMalloc(&s->d_nwork, sizeof(int)) || cudaMallocHost(&s->h_nwork, sizeof(int)))
+        cudaMalloc(&s->d_nwork, sizeof(int)) || cudaMallocHost(&s->h_nwork, sizeof(int)) ||
+        cudaMalloc(&s->d_counts, 2 * sizeof(int)) ||
+        cudaMallocHost(&s->h_counts, 2 * sizeof(int)) ||
+        cudaMalloc(&s->d_active, (size_t)max_slots * sizeof(int)) ||
+        cudaMallocHost(&s->h_active, (size_t)max_slots * sizeof(int)))
         return bail(fail(EB2_ENOMEM, "server allocation failed"));
     memset(s->h_desc, 0, (size_t)max_slots * sizeof(SlotDesc));
     if (cudaMemsetAsync(s->d_ctrl, 0, (size_t)max_slots * sizeof(Ctrl), s->stream) ||
@@ -376,6 +423,12 @@ int eb2_server_destroy(eb2_server* s) {
     cudaFreeHost(s->h_work);
     cudaFree(s->d_nwork);
     cudaFreeHost(s->h_nwork);
+    cudaFree(s->d_bcwork);
+    cudaFreeHost(s->h_bcwork);
+    cudaFree(s->d_counts);
+    cudaFreeHost(s->h_counts);
+    cudaFree(s->d_active);
+    cudaFreeHost(s->h_active);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return EB2_OK;

@@ -145,26 +145,38 @@ def test_mixed_near_vacuum_quadrant(gpu):
     pressure), moving diagonally into the other three, 128^2 to t = 0.1.  The
     shocks of the neighbouring quadrants run into near vacuum, where the mixed
     form projects with the FP64 eigenvector matrices.  It stays finite and
-    positive, follows the FP64 form in density (L1 as for the other runs) and
-    in the pressure of the near-vacuum region."""
+    positive and follows the FP64 form to within the spread that rounding of
+    FP32 size alone causes here: an FP64 run whose initial values are moved
+    by a seeded relative 2^-24 sets that floor, in density L1 and in the
+    pressure of the near-vacuum region, and the mixed form must stay within
+    twice it."""
     n = 128
     q = [1.5, 0.0, 0.0, 1.5, 0.5323, 1.206, 0.0, 0.3, 0.138, 1.206, 1.206, 1.0e-5,
          0.5323, 0.0, 1.206, 0.3]
     out = {}
-    for name in ("fp64", "mixed"):
+    for name in ("fp64", "mixed", "floor"):
         prec = gpu.lib.MIXED if name == "mixed" else gpu.lib.FP64
         with gpu.Solver(n, n, precision=prec, recon=5, characteristic=True,
                         weno_z=False) as s:
             s.init_case(gpu.lib.CASE_FOUR_QUADRANT, q)
+            if name == "floor":
+                U = s.download()
+                rng = np.random.default_rng(11)
+                inner = U[:, GC:-GC, GC:-GC]
+                inner *= 1.0 + rng.choice([-1.0, 1.0], size=inner.shape) * 2.0 ** -24
+                s.upload(U)
             s.run(3, 2, 1 / n, 1 / n, 0.1)
             assert s.status() == 0
             out[name] = interior(s.con_to_pri())
-    a, b = out["fp64"], out["mixed"]
+    a, b, f = out["fp64"], out["mixed"], out["floor"]
     vac = a[3] < 1e-3 * a[3].mean()
     assert vac.sum() > n * n // 10                     # the near-vacuum region is large
     assert np.all(np.isfinite(b)) and b[0].min() > 0 and b[3].min() > 0
-    rel_p = np.abs(b[3] - a[3])[vac] / a[3][vac]
-    print(f"near-vacuum quadrant: density L1 {np.mean(np.abs(b[0] - a[0])):.3e}, "
-          f"pressure there max rel {rel_p.max():.3e}")
-    assert rel_p.max() < 1e-3
-    assert float(np.mean(np.abs(b[0] - a[0]))) < L1_TOL
+    l1 = float(np.mean(np.abs(b[0] - a[0])))
+    l1_floor = float(np.mean(np.abs(f[0] - a[0])))
+    rel_p = float((np.abs(b[3] - a[3])[vac] / a[3][vac]).max())
+    rel_p_floor = float((np.abs(f[3] - a[3])[vac] / a[3][vac]).max())
+    print(f"near-vacuum quadrant: density L1 {l1:.3e} (floor {l1_floor:.3e}), pressure there "
+          f"max rel {rel_p:.3e} (floor {rel_p_floor:.3e})")
+    assert l1 < max(2.0 * l1_floor, L1_TOL)
+    assert rel_p < max(2.0 * rel_p_floor, 1e-4)
