@@ -453,16 +453,15 @@ def config(args):
 
 def measured_traffic(nx, precision, scheme):
     """DRAM bytes (read + write) per fused-stage launch of this workload, from
-    the committed ncu launch-list summary profiles/launches_<precision>_<nx>.md
-    (taken with the same bench command), or None when there is none."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                        f"launches_{precision}_{nx}.md")
+    the committed ncu summary profiles/traffic_<precision>_<nx>.md (taken with
+    the same bench command), or None when there is none."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{precision}_{nx}.md")
     if scheme != "hllc" or not os.path.exists(path):
         return None
     for line in open(path):
-        if "k_stage" in line and line.startswith("|"):
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            return (float(cells[4].split()[0]) + float(cells[5].split()[0])) * 1e6
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if line.startswith("|") and cells[0] == "traffic per launch":
+            return float(cells[1].split()[0]) * 1e6
     return None
 
 
@@ -478,8 +477,8 @@ def profile_rows(precision):
             continue
         cells = [c.strip() for c in line.strip().strip("|").split("|")]
         if cells[0] == "metric":
-            col = next((i for i, c in enumerate(cells) if c.startswith("now") or "(now)" in c),
-                       None)
+            col = next((i for i, c in enumerate(cells)
+                        if c.startswith("now") or "(now)" in c or c == "value"), None)
         elif col is not None and len(cells) > col:
             rows[cells[0]] = cells[col]
     return rows

@@ -108,23 +108,20 @@ EB2_HD double rcp64(double x) {
 #endif
 }
 
-// Per-cell primitive data kept in shared memory (FP32 values of FP64 results).
-enum : int { P_RHO = 0, P_U = 1, P_V = 2, P_P = 3, P_H = 4, P_SR = 5, NP = 6 };
+// Per-cell primitive data kept in shared memory (FP32 values of FP64 results):
+// a float4 (rho, u, v, p) and a float2 (h = gamma/(gamma-1) p/rho, sqrt(rho)),
+// so that an interface reads each cell's record with two vector loads.
 
 // Primitive record of one cell from its conserved state (q in FP64, qf the
 // same values rounded to FP32): the pressure is formed in FP64, where E minus
 // the kinetic energy cancels in low-pressure flows, then stored FP32; the
 // velocities, enthalpy and sqrt(rho) need only FP32.
-EB2_HD void cell_prims(const double* q, const float* qf, const Gas& g, float* P, int ps) {
+EB2_HD void cell_prims(const double* q, const float* qf, const Gas& g, float4* P, float2* H) {
     const double ir = rcp64(q[0]);
     const double p = fma(-0.5 * ir, fma(q[1], q[1], q[2] * q[2]), q[3]) * g.gm1;
     const float pf = (float)p, irf = rcp(qf[0]);
-    P[P_RHO * ps] = qf[0];
-    P[P_U * ps] = qf[1] * irf;
-    P[P_V * ps] = qf[2] * irf;
-    P[P_P * ps] = pf;
-    P[P_H * ps] = (float)g.gr * pf * irf;
-    P[P_SR * ps] = sqr(qf[0]);
+    *P = make_float4(qf[0], qf[1] * irf, qf[2] * irf, pf);
+    *H = make_float2((float)g.gr * pf * irf, sqr(qf[0]));
 }
 
 // Eigen-system parameters at an interface (the Roe average), in the form the
@@ -152,16 +149,15 @@ EB2_HD Eig eig_from(float u, float v, float c2, float gm1) {
 
 // Roe average from FP32 cell data: weights sqrt(rho), sound speed from the
 // cell enthalpies h (no H - q^2/2 cancellation).
-EB2_HD Eig roe_f32(const float* a, const float* b, int ps, float gm1) {
-    float sa = a[P_SR * ps], sb = b[P_SR * ps];
-    float rs = rcp(sa + sb);
-    float wa = sa * rs, wb = sb * rs;
-    float ua = a[P_U * ps], ub = b[P_U * ps], va = a[P_V * ps], vb = b[P_V * ps];
-    float u = wa * ua + wb * ub;
-    float v = wa * va + wb * vb;
-    float du = ua - ub, dv = va - vb;
-    float h = wa * a[P_H * ps] + wb * b[P_H * ps];
-    float c2 = gm1 * (h + 0.5f * wa * wb * (du * du + dv * dv));
+EB2_HD Eig roe_f32(const float4& a, const float2& ha, const float4& b, const float2& hb,
+                   float gm1) {
+    const float rs = rcp(ha.y + hb.y);
+    const float wa = ha.y * rs, wb = hb.y * rs;
+    const float u = wa * a.y + wb * b.y;
+    const float v = wa * a.z + wb * b.z;
+    const float du = a.y - b.y, dv = a.z - b.z;
+    const float h = wa * ha.x + wb * hb.x;
+    const float c2 = gm1 * (h + 0.5f * wa * wb * (du * du + dv * dv));
     return eig_from(u, v, c2, gm1);
 }
 

@@ -5,10 +5,17 @@
 // tile needs and applies flux difference + RK combination to its cells.
 // Differences: the staged tile is FP32, per-cell primitives come from FP64
 // arithmetic, interface work is FP32 in delta form (eb2_point_mixed.cuh), the
-// fluxes are widened to FP64 in shared memory, and the flux difference and
+// fluxes are widened to FP64 where they are read, and the flux difference and
 // RK combination are FP64 with the stage input re-read in FP64.
 // Reconstruction: WENO5 in characteristic variables (Jiang-Shu or WENO-Z
 // weights).
+//
+// Shared memory holds every per-cell and per-face record as one vector
+// (float4 conserved state, float4 + float2 primitives, float4 face flux), so
+// that a stencil point, a primitive record or a flux is one 16-byte load: the
+// warp's 32 consecutive cells then cover four 128-byte wavefronts without
+// bank conflicts, and the interfaces issue a quarter of the shared-memory
+// instructions of a field-per-array layout.
 #pragma once
 
 #include <type_traits>
@@ -34,9 +41,10 @@ constexpr int PS = PX * PY;
 constexpr int XS = (TX + 1) * TY;
 constexpr int YS = TX * (TY + 1);
 constexpr int NJX = (TX + 1) * TY, NJY = TX * (TY + 1);
-// FP32 tile and primitives, FP64 interface fluxes (widened exactly once, so
-// that flux differences telescope and the step conserves to FP64 round-off)
-constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS + 4 * XS + 4 * YS) * sizeof(float);
+// FP32 face fluxes (widened exactly where read, so that both cells of a face
+// see the same value, the flux differences telescope and the step conserves
+// to FP64 round-off), FP32 tile, FP32 primitives
+constexpr size_t SMEM = (size_t)(XS + YS + FS + PS) * sizeof(float4) + (size_t)PS * sizeof(float2);
 
 // Conserved differences of both sides of an interface next to a near-vacuum
 // cell: the stencil's six cells are read in FP64 from the stage input (cell i at
@@ -44,8 +52,10 @@ constexpr size_t SMEM = (size_t)(4 * FS + f32::NP * PS + 4 * XS + 4 * YS) * size
 // eigenvector matrices are the reference's, in FP64 (Characteriz.h:333-392 for
 // x, :435-494 for y), and so are the projections of the differences onto them
 // and the back-projection; only the WENO weights and candidate values between
-// the two run in FP32 lanes, as on every other interface.  Rare, so kept out
-// of line: its FP64 arrays do not weigh on the registers of the common path.
+// the two run in FP32 lanes, as on every other interface.  Rare: the stage
+// kernel runs these interfaces in a pass of their own after the others, so
+// that their FP64 arithmetic does not weigh on the registers of the common
+// path.
 template <int DIR, bool WZ>
 __host__ __device__ __noinline__ void vacuum_delta(const double* __restrict__ u, size_t g2,
                                           long long step, size_t plane, const Gas g,
@@ -100,37 +110,35 @@ __host__ __device__ __noinline__ void vacuum_delta(const double* __restrict__ u,
 
 // Is either cell next to an interface near vacuum (p below pthr, 1e-3 of the
 // mean pressure)?
-EB2_HD bool near_vacuum(const float* pa, const float* pb, float pthr) {
-    return pa[f32::P_P * PS] < pthr || pb[f32::P_P * PS] < pthr;
-}
+EB2_HD bool near_vacuum(float pa, float pb, float pthr) { return pa < pthr || pb < pthr; }
 
-// One interface.  s: stencil cell n = 0 of field 0 (fields FS apart, `stride`
-// along the sweep); pa/pb: primitive records of cells i and i+1 (fields PS
-// apart); ga/gb: the two cells in global memory.  VAC: an interface next to a
-// near-vacuum cell, whose characteristic projections take FP64 matrices
-// (vacuum_delta).
+// One interface.  s: stencil cell n = 0 (i-2), `stride` records along the
+// sweep; pa/ha and pb/hb: primitive records of cells i and i+1; ga/gb: the
+// two cells in global memory.  VAC: an interface next to a near-vacuum cell,
+// whose characteristic projections take FP64 matrices (vacuum_delta).
 template <bool VAC, int DIR, bool WZ, int FLUX>
-EB2_HD unsigned face_flux(const float* __restrict__ s, int stride, const float* __restrict__ pa,
-                          const float* __restrict__ pb, const double* __restrict__ u, size_t ga,
-                          size_t gb, size_t plane, const Gas& g, int positivity,
-                          float* __restrict__ out, int ostride) {
+EB2_HD unsigned face_flux(const float4* __restrict__ s, int stride,
+                          const float4* __restrict__ pa, const float2* __restrict__ ha,
+                          const float4* __restrict__ pb, const float2* __restrict__ hb,
+                          const double* __restrict__ u, size_t ga, size_t gb, size_t plane,
+                          const Gas& g, int positivity, float4* __restrict__ out) {
     const float gm1 = (float)g.gm1, gamma = (float)g.gamma;
-    const float b3 = s[3 * FS + 2 * stride];
     f32::f2 dq[4];
     if constexpr (VAC) {
         vacuum_delta<DIR, WZ>(u, ga, (long long)gb - (long long)ga, plane, g, dq);
     } else {
-        const f32::Eig e = f32::roe_f32(pa, pb, PS, gm1);
-        const float b0 = s[2 * stride], b1 = s[FS + 2 * stride], b2 = s[2 * FS + 2 * stride];
+        // (the primitive records are read where they are used, so that they
+        // hold no registers across the reconstruction)
+        const float4 base = s[2 * stride];
+        const f32::Eig e = f32::roe_f32(*pa, *ha, *pb, *hb, gm1);
         // characteristic differences y_n = L (U_n - U_i), n = i-2..i+3 (y_2 = 0)
         float y[4][6];
 #pragma unroll
         for (int n = 0; n < 6; n++) {
             if (n == 2) continue;
-            float d0 = s[n * stride] - b0, d1 = s[FS + n * stride] - b1;
-            float d2 = s[2 * FS + n * stride] - b2, d3 = s[3 * FS + n * stride] - b3;
+            const float4 q = s[n * stride];
             float c[4];
-            f32::project<DIR>(e, d0, d1, d2, d3, c);
+            f32::project<DIR>(e, q.x - base.x, q.y - base.y, q.z - base.z, q.w - base.w, c);
 #pragma unroll
             for (int k = 0; k < 4; k++) y[k][n] = c[k];
         }
@@ -156,19 +164,18 @@ EB2_HD unsigned face_flux(const float* __restrict__ s, int stride, const float* 
         f32::unproject2<DIR>(e, W, dq);
     }
     // minus side around cell i, plus side around cell i+1
-    const float ra = pa[f32::P_RHO * PS], ua = pa[f32::P_U * PS], va = pa[f32::P_V * PS],
-                pas = pa[f32::P_P * PS];
-    const float rb = pb[f32::P_RHO * PS], ub = pb[f32::P_U * PS], vb = pb[f32::P_V * PS],
-                pbs = pb[f32::P_P * PS], eb = s[3 * FS + 3 * stride];
+    const float4 A = *pa, B = *pb;
+    const float ea = s[2 * stride].w, eb = s[3 * stride].w;
     f32::Prim L, R;
-    f32::prim_from_delta2<DIR>(make_float2(ra, rb), make_float2(ua, ub), make_float2(va, vb),
-                               make_float2(pas, pbs), make_float2(b3, eb), dq, gm1, L, R);
+    f32::prim_from_delta2<DIR>(make_float2(A.x, B.x), make_float2(A.y, B.y),
+                               make_float2(A.z, B.z), make_float2(A.w, B.w),
+                               make_float2(ea, eb), dq, gm1, L, R);
     unsigned st = 0;
     if (!(L.r > 0.0f && L.p > 0.0f && R.r > 0.0f && R.p > 0.0f)) {
         if (positivity) {
             float z[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            L = f32::prim_from_delta<DIR>(ra, ua, va, pas, b3, z, gm1);
-            R = f32::prim_from_delta<DIR>(rb, ub, vb, pbs, eb, z, gm1);
+            L = f32::prim_from_delta<DIR>(A.x, A.y, A.z, A.w, ea, z, gm1);
+            R = f32::prim_from_delta<DIR>(B.x, B.y, B.z, B.w, eb, z, gm1);
         } else {
             st |= ST_NONPHYSICAL;
         }
@@ -182,25 +189,23 @@ EB2_HD unsigned face_flux(const float* __restrict__ s, int stride, const float* 
     else if (FLUX == FLUX_ROEHC) f32::roehc(L, R, gamma, F);
     else f32::llf(L, R, gamma, F);
     // (mass, normal, tangential, energy) -> (rho, rho u, rho v, rho E)
-    out[0] = F[0];
-    out[ostride] = DIR == 1 ? F[1] : F[2];
-    out[2 * ostride] = DIR == 1 ? F[2] : F[1];
-    out[3 * ostride] = F[3];
+    *out = make_float4(F[0], DIR == 1 ? F[1] : F[2], DIR == 1 ? F[2] : F[1], F[3]);
     return st;
 }
 
 // Both paths, chosen per interface (the CPU checks of the face arithmetic).
 template <int DIR, bool WZ, int FLUX>
-EB2_HD unsigned interface_flux(const float* __restrict__ s, int stride,
-                               const float* __restrict__ pa, const float* __restrict__ pb,
+EB2_HD unsigned interface_flux(const float4* __restrict__ s, int stride,
+                               const float4* __restrict__ pa, const float2* __restrict__ ha,
+                               const float4* __restrict__ pb, const float2* __restrict__ hb,
                                const double* __restrict__ u, size_t ga, size_t gb, size_t plane,
-                               float pthr, const Gas& g, int positivity, float* __restrict__ out,
-                               int ostride) {
-    if (near_vacuum(pa, pb, pthr))
-        return face_flux<true, DIR, WZ, FLUX>(s, stride, pa, pb, u, ga, gb, plane, g, positivity,
-                                              out, ostride);
-    return face_flux<false, DIR, WZ, FLUX>(s, stride, pa, pb, u, ga, gb, plane, g, positivity,
-                                           out, ostride);
+                               float pthr, const Gas& g, int positivity,
+                               float4* __restrict__ out) {
+    if (near_vacuum(pa->w, pb->w, pthr))
+        return face_flux<true, DIR, WZ, FLUX>(s, stride, pa, ha, pb, hb, u, ga, gb, plane, g,
+                                              positivity, out);
+    return face_flux<false, DIR, WZ, FLUX>(s, stride, pa, ha, pb, hb, u, ga, gb, plane, g,
+                                           positivity, out);
 }
 
 // One tile (ti, tj) of one stage; shared by the single-solve and batched kernels.
@@ -208,11 +213,12 @@ template <bool WZ, int FLUX>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, int tiles_x) {
     Ctrl* ctrl = a.ctrl;
     if (!ctrl->active) return;
-    extern __shared__ float smf[];
-    float* sFx = smf;
-    float* sFy = sFx + 4 * XS;
-    float* sU = sFy + 4 * YS;
-    float* sP = sU + 4 * FS;
+    extern __shared__ float4 smv[];
+    float4* sFx = smv;
+    float4* sFy = sFx + XS;
+    float4* sU = sFy + YS;
+    float4* sP = sU + FS;
+    float2* sH = reinterpret_cast<float2*>(sP + PS);
     __shared__ double red[3][NT / 32];
 
     const int rows = a.grid.rows, cols = a.grid.cols;
@@ -223,33 +229,40 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     const float pthr = (float)(1.0e-3 * ctrl->pmean);
 
     // 1. tile + halo as FP32; primitives of the tile and its first ring from FP64.
-    // Thread t takes elements t, t + NT, ... of the HX x HY tile, its (row,
-    // column) stepped without divisions.
+    // Thread t takes elements t, t + NT, ... of the HX x HY tile; all of its
+    // loads are issued before any is used, so their latencies overlap.
     {
+        constexpr int NE = (FS + NT - 1) / NT;
+        double q[NE][4];
         int r = threadIdx.x / HY, c = threadIdx.x - r * HY;
-        for (int e = threadIdx.x; e < FS; e += NT) {
+        int er[NE], ec[NE];
+#pragma unroll
+        for (int t = 0; t < NE; t++) {
+            er[t] = r;
+            ec[t] = c;
             const int i = i0 - 3 + r, j = j0 - 3 + c;
-            double q[4] = {0.0, 0.0, 0.0, 0.0};
-            if (i < rows && j < cols) {
-                const double* src = uin + (size_t)i * cols + j;
+            const bool in = threadIdx.x + t * NT < FS && i < rows && j < cols;
+            const double* src = uin + (in ? (size_t)i * cols + j : 0);
 #pragma unroll
-                for (int k = 0; k < 4; k++) q[k] = src[k * plane];
-            }
-            float qf[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                qf[k] = (float)q[k];
-                sU[k * FS + e] = qf[k];
-            }
-            const int pr = r - 2, pc = c - 2;
-            if ((unsigned)pr < (unsigned)PX && (unsigned)pc < (unsigned)PY)
-                f32::cell_prims(q, qf, g, sP + pr * PY + pc, PS);
+            for (int k = 0; k < 4; k++) q[t][k] = in ? src[k * plane] : 0.0;
             c += NT % HY;
             r += NT / HY;
             if (c >= HY) {
                 c -= HY;
                 r++;
             }
+        }
+#pragma unroll
+        for (int t = 0; t < NE; t++) {
+            const int e = threadIdx.x + t * NT;
+            if (e >= FS) break;
+            float qf[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) qf[k] = (float)q[t][k];
+            sU[e] = make_float4(qf[0], qf[1], qf[2], qf[3]);
+            const int pr = er[t] - 2, pc = ec[t] - 2;
+            if ((unsigned)pr < (unsigned)PX && (unsigned)pc < (unsigned)PY)
+                f32::cell_prims(q[t], qf, g, sP + pr * PY + pc, sH + pr * PY + pc);
         }
     }
     __syncthreads();
@@ -266,22 +279,23 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
             int rr = job / TY, cc = job - rr * TY;
             int i = i0 - 1 + rr, j = j0 + cc;
             if (i >= rows - GC || j >= cols - GC) return 0u;  // past the domain edge
+            const int pa = rr * PY + (cc + 1);
+            if (!VAC && near_vacuum(sP[pa].w, sP[pa + PY].w, pthr)) return ~0u;
             size_t ga = (size_t)i * cols + j;
-            const float* pa = sP + rr * PY + (cc + 1);
-            if (!VAC && near_vacuum(pa, pa + PY, pthr)) return ~0u;
-            return face_flux<VAC, 1, WZ, FLUX>(sU + rr * HY + (cc + 3), HY, pa, pa + PY, uin,
-                                               ga, ga + cols, plane, g, pos,
-                                               sFx + rr * TY + cc, XS);
+            return face_flux<VAC, 1, WZ, FLUX>(sU + rr * HY + (cc + 3), HY, sP + pa, sH + pa,
+                                               sP + pa + PY, sH + pa + PY, uin, ga, ga + cols,
+                                               plane, g, pos, sFx + rr * TY + cc);
         }
         int q = job - NJX;
         int rr = q / (TY + 1), cc = q - rr * (TY + 1);
         int i = i0 + rr, j = j0 - 1 + cc;
         if (i >= rows - GC || j >= cols - GC) return 0u;
+        const int pa = (rr + 1) * PY + cc;
+        if (!VAC && near_vacuum(sP[pa].w, sP[pa + 1].w, pthr)) return ~0u;
         size_t ga = (size_t)i * cols + j;
-        const float* pa = sP + (rr + 1) * PY + cc;
-        if (!VAC && near_vacuum(pa, pa + 1, pthr)) return ~0u;
-        return face_flux<VAC, 2, WZ, FLUX>(sU + (rr + 3) * HY + cc, 1, pa, pa + 1, uin, ga,
-                                           ga + 1, plane, g, pos, sFy + rr * (TY + 1) + cc, YS);
+        return face_flux<VAC, 2, WZ, FLUX>(sU + (rr + 3) * HY + cc, 1, sP + pa, sH + pa,
+                                           sP + pa + 1, sH + pa + 1, uin, ga, ga + 1, plane, g,
+                                           pos, sFy + rr * (TY + 1) + cc);
     };
     for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++) {
         const unsigned r = face(std::false_type{}, job);
@@ -294,31 +308,53 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
         __syncthreads();
     }
 
-    // 3. flux difference (widened to FP64), RK combination in FP64
+    // 3. flux difference (widened to FP64), RK combination in FP64.  The
+    // thread's cells (TX TY / NT of them) load their stage input and step
+    // start state first, then combine.
     const double dt = ctrl->dt;
     const double idx = a.grid.inv_dx, idy = a.grid.inv_dy;
     const double grav = a.num.gravity;
     double mx = 0.0, my = 0.0, ps = 0.0;
-    for (int e = threadIdx.x; e < TX * TY; e += NT) {
-        int rr = e / TY, cc = e - rr * TY;
-        int i = i0 + rr, j = j0 + cc;
-        if (i >= rows - GC || j >= cols - GC) continue;
-        size_t o = (size_t)i * cols + j;
-        double x[4], src[4] = {0.0, 0.0, 0.0, 0.0}, out[4];
+    constexpr int NC = TX * TY / NT;
+    static_assert(TX * TY % NT == 0, "whole cells per thread");
+    double xs[NC][4], ys[NC][4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) x[k] = uin[o + k * plane];
+    for (int t = 0; t < NC; t++) {
+        const int e = threadIdx.x + t * NT;
+        const int rr = e / TY, cc = e - rr * TY;
+        const int i = i0 + rr, j = j0 + cc;
+        const bool in = i < rows - GC && j < cols - GC;
+        const size_t o = in ? (size_t)i * cols + j : 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            xs[t][k] = in ? uin[o + k * plane] : 0.0;
+            ys[t][k] = in && a.combine != COMB_EULER ? a.un[o + k * plane] : xs[t][k];
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NC; t++) {
+        const int e = threadIdx.x + t * NT;
+        const int rr = e / TY, cc = e - rr * TY;
+        const int i = i0 + rr, j = j0 + cc;
+        if (i >= rows - GC || j >= cols - GC) continue;
+        const size_t o = (size_t)i * cols + j;
+        const double* x = xs[t];
+        double src[4] = {0.0, 0.0, 0.0, 0.0}, out[4];
         if (a.num.source) {
             double rho = x[0];
             src[2] = rho * grav;
             src[3] = rho * grav * (x[2] / rho);
         }
+        // widened exactly; both cells of a face read the same FP32 value
+        const float4 fxp = sFx[(rr + 1) * TY + cc], fxm = sFx[rr * TY + cc];
+        const float4 fyp = sFy[rr * (TY + 1) + cc + 1], fym = sFy[rr * (TY + 1) + cc];
+        const float fp[4] = {fxp.x, fxp.y, fxp.z, fxp.w}, fm[4] = {fxm.x, fxm.y, fxm.z, fxm.w};
+        const float gp[4] = {fyp.x, fyp.y, fyp.z, fyp.w}, gm[4] = {fym.x, fym.y, fym.z, fym.w};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            // widened exactly; both cells of a face read the same FP32 value
-            double fxp = sFx[k * XS + (rr + 1) * TY + cc], fxm = sFx[k * XS + rr * TY + cc];
-            double fyp = sFy[k * YS + rr * (TY + 1) + cc + 1], fym = sFy[k * YS + rr * (TY + 1) + cc];
-            double L = -(fxp - fxm) * idx - (fyp - fym) * idy + src[k];
-            double y = a.combine == COMB_EULER ? x[k] : a.un[o + k * plane];
+            double L = -((double)fp[k] - (double)fm[k]) * idx - ((double)gp[k] - (double)gm[k]) * idy +
+                       src[k];
+            const double y = ys[t][k];
             double r;
             switch (a.combine) {
                 case COMB_EULER: r = y + dt * L; break;

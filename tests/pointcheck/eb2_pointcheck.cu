@@ -27,23 +27,29 @@ unsigned fp64_face(const double* cells, double delta, const Gas& g, int pos, dou
 
 template <int DIR, bool WZ, int FLUX>
 unsigned mixed_face(const double* cells, double pthr, const Gas& g, int pos, double* F) {
-    static float sU[4 * mixstage::FS], sP[f32::NP * mixstage::PS];
+    float4 sU[6];
     for (int n = 0; n < 6; n++)
-        for (int k = 0; k < 4; k++) sU[k * mixstage::FS + n] = (float)cells[4 * n + k];
+        sU[n] = make_float4((float)cells[4 * n], (float)cells[4 * n + 1], (float)cells[4 * n + 2],
+                            (float)cells[4 * n + 3]);
     // the six cells in FP64 as the kernel's near-vacuum path reads them from
     // the stage input: field planes of 6 values, cell i at index 2
     double u[24];
     for (int n = 0; n < 6; n++)
         for (int k = 0; k < 4; k++) u[n + 6 * k] = cells[4 * n + k];
+    float4 P[2];
+    float2 H[2];
     for (int c = 0; c < 2; c++) {
         float qf[4];
         for (int k = 0; k < 4; k++) qf[k] = (float)cells[4 * (2 + c) + k];
-        f32::cell_prims(cells + 4 * (2 + c), qf, g, sP + c, mixstage::PS);
+        f32::cell_prims(cells + 4 * (2 + c), qf, g, P + c, H + c);
     }
-    float Ff[4];
-    unsigned st = mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, sP, sP + 1, u, 2, 3, 6,
-                                                          (float)pthr, g, pos, Ff, 1);
-    for (int k = 0; k < 4; k++) F[k] = Ff[k];
+    float4 Ff;
+    unsigned st = mixstage::interface_flux<DIR, WZ, FLUX>(sU, 1, P, H, P + 1, H + 1, u, 2, 3, 6,
+                                                          (float)pthr, g, pos, &Ff);
+    F[0] = Ff.x;
+    F[1] = Ff.y;
+    F[2] = Ff.z;
+    F[3] = Ff.w;
     return st;
 }
 
