@@ -57,7 +57,7 @@ constexpr size_t SMEM = (size_t)(XS + YS + FS + PS) * sizeof(float4) + (size_t)P
 // that their FP64 arithmetic does not weigh on the registers of the common
 // path.
 template <int DIR, bool WZ>
-__host__ __device__ __noinline__ void vacuum_delta(const double* __restrict__ u, size_t g2,
+EB2_HD void vacuum_delta(const double* __restrict__ u, size_t g2,
                                           long long step, size_t plane, const Gas g,
                                           f32::f2* dq) {
     // the two cells next to the interface stay in registers; the other four
