@@ -43,10 +43,13 @@ CUDA_SOURCES = [
     ("eb2_server.cu", True),
     ("eb2_stage_mixed.cu", False),
     ("eb2_batch_mixed.cu", False),
+    ("eb2_batch_mixed_s8.cu", False),
+    ("eb2_batch_mixed_s32.cu", False),
 ]
 C_SOURCES = ["eb2_control.c", "rpf_runtime.c"]
 HEADERS = ["eb2_common.cuh", "eb2_kernels.h", "eb2_fdiv.cuh", "eb2_point_fp64.cuh", "eb2_stage_fp64.cuh",
-           "eb2_point_mixed.cuh", "eb2_stage_mixed.cuh", "eb2_loop.cuh", "eb2_batch.cuh"]
+           "eb2_point_mixed.cuh", "eb2_stage_mixed.cuh", "eb2_loop.cuh", "eb2_batch.cuh",
+           "eb2_batch_mixed.cuh"]
 
 
 def _nvcc() -> str:

@@ -14,6 +14,11 @@
 
 namespace eb2 {
 
+// Tile shapes the batched mixed kernels come in (eb2_stage_mixed.cuh: 16 x 32
+// cells and 256 threads, 8 x 32 and 128, 32 x 32 and 512); an FP64 server has
+// one, the FP64 form's 15 x 32.
+constexpr int kMixedShapes = 3;
+
 struct SlotDesc {
     double* u;            // state
     double* u1;           // stage 1 output
@@ -24,8 +29,8 @@ struct SlotDesc {
     Gas gas;
     Numerics num;
     Boundary bnd;
-    int tiles_x;          // tiles along y
-    int ntiles;
+    int tiles_x;          // tiles along y (32 columns in every shape)
+    int ntiles[kMixedShapes];  // tiles of the slot in each tile shape
     int ncells;
     int bc_blocks;        // ghost-fill blocks of this slot (its entries in the bc work list)
 };
@@ -68,6 +73,7 @@ struct BatchLaunch {
     int active_grid;         // blocks of the end-of-step reduction (>= *nactive)
     int each = 0;            // 1: one CTA per work item (grid >= every work-list
                              // length it is used with), 0: persistent CTAs that loop
+    int shape = 0;           // tile shape of the stage kernels (index into the shapes)
 };
 cudaError_t launch_stage_batch_fp64(const BatchLaunch& b, const Numerics& num, int stage,
                                     cudaStream_t s);
@@ -75,6 +81,10 @@ cudaError_t launch_stage_batch_mixed(const BatchLaunch& b, const Numerics& num, 
                                      cudaStream_t s);
 cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s);
 cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s);
-int stage_batch_max_blocks_per_sm(int precision);
+// Tile shapes of a server's stage kernels (1 for FP64, kMixedShapes for the
+// mixed form), their tile rows, and their resident CTAs per SM.
+int batch_shapes(int precision);
+int batch_shape_tile_x(int precision, int shape);
+int stage_batch_max_blocks_per_sm(int precision, int shape);
 
 }  // namespace eb2

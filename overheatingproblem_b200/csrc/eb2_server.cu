@@ -64,13 +64,24 @@ int fail(int code, const char* fmt, ...) {
             return fail(EB2_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_));             \
     } while (0)
 
-size_t slot_bytes(int nx, int ny) {
+// Tiles of an nx x ny slot in tile shape `shape` (32 columns per tile in
+// every shape).
+int slot_tiles(int nx, int ny, int precision, int shape) {
+    const int tx = batch_shape_tile_x(precision, shape);
+    return ((ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y) * ((nx + tx - 1) / tx);
+}
+
+// Partials of a slot: one triple per tile in the shape with the most tiles.
+int slot_partials(int nx, int ny, int precision) {
+    int n = 296;
+    for (int k = 0; k < batch_shapes(precision); k++)
+        n = std::max(n, slot_tiles(nx, ny, precision, k));
+    return n;
+}
+
+size_t slot_bytes(int nx, int ny, int precision) {
     size_t n = (size_t)4 * (nx + 2 * GC) * (ny + 2 * GC) * sizeof(double);
-    Grid g{};
-    g.nx = nx;
-    g.ny = ny;
-    int tiles = std::max(stage_blocks_max(g), 296);
-    return 3 * n + (size_t)3 * tiles * sizeof(double);
+    return 3 * n + (size_t)3 * slot_partials(nx, ny, precision) * sizeof(double);
 }
 
 double now_s() {
@@ -98,7 +109,10 @@ struct eb2_server {
     int* d_nwork = nullptr;
     int* h_nwork = nullptr;       // pinned
     int work_cap = 0;
-    int nwork = 0;
+    int nwork = 0;                // work-list length in the current tile shape
+    int nwork0 = 0;               // the same in shape 0 (the batch-shape class)
+    int shape = 0;                // tile shape the work list is built for
+    int nshapes = 1;
     int2* d_bcwork = nullptr;     // ghost-fill work list: (slot, block of the slot)
     int2* h_bcwork = nullptr;     // pinned
     int* d_counts = nullptr;      // device: ghost-fill and active-slot list lengths
@@ -110,7 +124,7 @@ struct eb2_server {
     long long next_id = 0;
     int sms = 148;
     std::map<int, cudaGraphExec_t> graphs;   // launch key (grid_key) -> graph
-    std::map<int, int> tuned;                // shape class -> launch key
+    std::map<int, int> tuned;                // batch-shape class -> launch key
     int bc_grid = 8;                         // blocks of the ghost-fill launches
     int active_grid = 8;                     // blocks of the end-of-step launches
     long long graph_launches = 0;
@@ -128,9 +142,10 @@ cudaError_t stage_batch(eb2_server* s, const BatchLaunch& b, int stage) {
                                      : launch_stage_batch_fp64(b, s->num, stage, s->stream);
 }
 
-// A stage-kernel launch shape: `grid` CTAs, looping over the work list
-// (each = 0) or one per work item (each = 1, grid >= the work-list length).
-int grid_key(int grid, int each) { return 2 * grid + each; }
+// A stage-kernel launch shape: tile shape `shape`, `grid` CTAs looping over the
+// work list (each = 0) or one per work item (each = 1, grid >= the work-list
+// length).
+int grid_key(int shape, int grid, int each) { return (shape << 24) | (2 * grid + each); }
 
 int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
     auto it = s->graphs.find(key);
@@ -141,8 +156,9 @@ int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
     BatchLaunch b{s->d_desc, s->nslots, s->d_work, s->d_nwork, 0,
                   s->d_bcwork, s->d_counts, s->bc_grid,
                   s->d_active, s->d_counts + 1, s->active_grid};
+    b.shape = key >> 24;
     CKS(stage_batch(s, b, 0));  // kernel attributes, outside the capture
-    b.grid = key / 2;
+    b.grid = (key & 0xffffff) / 2;
     b.each = key % 2;
     cudaGraph_t g = nullptr;
     CKS(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -170,9 +186,13 @@ int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
 
 // Rewrite the work list and descriptors after admissions and retirements.
 int rebuild(eb2_server* s) {
-    int n = 0;
+    int n = 0, n0 = 0;
     for (int q = 0; q < s->nslots; q++)
-        if (s->slots[q].used && !s->slots[q].done) n += s->h_desc[q].ntiles;
+        if (s->slots[q].used && !s->slots[q].done) {
+            n += s->h_desc[q].ntiles[s->shape];
+            n0 += s->h_desc[q].ntiles[0];
+        }
+    s->nwork0 = n0;
     if (n > s->work_cap) {
         int cap = std::max(n, 2 * s->work_cap);
         if (s->d_work) CKS(cudaFreeAsync(s->d_work, s->stream));
@@ -225,7 +245,7 @@ int rebuild(eb2_server* s) {
     int w = 0;
     for (int q = 0; q < s->nslots; q++) {
         if (!s->slots[q].used || s->slots[q].done) continue;
-        for (int t = 0; t < s->h_desc[q].ntiles; t++) s->h_work[w++] = make_int2(q, t);
+        for (int t = 0; t < s->h_desc[q].ntiles[s->shape]; t++) s->h_work[w++] = make_int2(q, t);
     }
     *s->h_nwork = w;
     s->nwork = w;
@@ -258,52 +278,67 @@ int shape_class(int nwork) {
     return c;
 }
 
+// Switch the work list to tile shape `shape`.
+int use_shape(eb2_server* s, int shape) {
+    if (shape == s->shape && !s->dirty) return EB2_OK;
+    s->shape = shape;
+    return rebuild(s);
+}
+
 // One graph launch (kStepsPerGraph batch steps) with the tuned launch shape.
+// The autotuner times, per batch-shape class (log2 of the work-list length in
+// tile shape 0), every tile shape of the server's form and, per tile shape,
+// persistent grids of 1..CTAS CTAs per SM smaller than the work list and one
+// CTA per work item; the fastest is kept for the class.
 int launch_steps(eb2_server* s) {
-    const int maxb = stage_batch_max_blocks_per_sm(s->precision == EB2_MIXED ? 1 : 0);
-    const int cls = shape_class(s->nwork);
+    const int prec = s->precision == EB2_MIXED ? 1 : 0;
+    const int cls = shape_class(s->nwork0);
     auto it = s->tuned.find(cls);
     if (it == s->tuned.end()) {
-        // autotune: time each grid candidate on this batch; the
-        // slots advance during the trials, which is ordinary progress
+        // the slots advance during the trials, which is ordinary progress
         int best = 0;
         float best_ms = 1e30f;
         cudaEvent_t e0, e1;
         CKS(cudaEventCreate(&e0));
         CKS(cudaEventCreate(&e1));
-        // candidates: persistent grids of 1..maxb CTAs per SM smaller than the
-        // work list, and one CTA per work item (the hardware then hands tiles to
-        // SMs as they free up) over 2^cls CTAs, which covers every work-list
-        // length of this shape class
-        std::vector<int> keys;
-        for (int mult = 1; mult <= maxb; mult++)
-            if (mult * s->sms < s->nwork) keys.push_back(grid_key(mult * s->sms, 0));
-        keys.push_back(grid_key(1 << cls, 1));
-        for (int key : keys) {
-            cudaGraphExec_t ex;
-            if (int r = get_graph(s, key, &ex)) return r;
-            // one untimed launch first: the first launch of a new graph also
-            // uploads it, which would bias the comparison by more than the
-            // candidates differ
-            CKS(cudaGraphLaunch(ex, s->stream));
-            s->graph_launches++;
-            CKS(cudaEventRecord(e0, s->stream));
-            CKS(cudaGraphLaunch(ex, s->stream));
-            CKS(cudaEventRecord(e1, s->stream));
-            CKS(cudaEventSynchronize(e1));
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            s->graph_launches++;
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = key;
+        for (int sh = 0; sh < s->nshapes; sh++) {
+            if (int r = use_shape(s, sh)) return r;
+            // one CTA per work item over 2^k CTAs covers every work-list length
+            // of this class in this shape (an 8-row tile shape has up to twice
+            // the tiles of shape 0, a 32-row one at most as many)
+            const int each_grid = 1 << (cls + (batch_shape_tile_x(prec, sh) <
+                                               batch_shape_tile_x(prec, 0) ? 1 : 0));
+            std::vector<int> keys;
+            for (int mult = 1; mult <= stage_batch_max_blocks_per_sm(prec, sh); mult++)
+                if (mult * s->sms < s->nwork) keys.push_back(grid_key(sh, mult * s->sms, 0));
+            keys.push_back(grid_key(sh, each_grid, 1));
+            for (int key : keys) {
+                cudaGraphExec_t ex;
+                if (int r = get_graph(s, key, &ex)) return r;
+                // one untimed launch first: the first launch of a new graph also
+                // uploads it, which would bias the comparison by more than the
+                // candidates differ
+                CKS(cudaGraphLaunch(ex, s->stream));
+                s->graph_launches++;
+                CKS(cudaEventRecord(e0, s->stream));
+                CKS(cudaGraphLaunch(ex, s->stream));
+                CKS(cudaEventRecord(e1, s->stream));
+                CKS(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                s->graph_launches++;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = key;
+                }
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         s->tuned[cls] = best;
-        return EB2_OK;
+        return use_shape(s, best >> 24);
     }
+    if (int r = use_shape(s, it->second >> 24)) return r;
     cudaGraphExec_t ex;
     if (int r = get_graph(s, it->second, &ex)) return r;
     CKS(cudaGraphLaunch(ex, s->stream));
@@ -374,6 +409,7 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
                   : scheme == 33 ? FLUX_ROEHC
                                  : FLUX_LLF;
     s->gamma = gamma;
+    s->nshapes = batch_shapes(precision == EB2_MIXED ? 1 : 0);
     s->budget = hbm_budget_bytes;
     s->nslots = max_slots;
     s->slots.resize(max_slots);
@@ -450,7 +486,7 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
         if ((bc[q] == BC_PERIODIC || (bc[q] == BC_REFLECT && (q == 0 || q == 3))) && n < GC)
             return fail(EB2_EUNSUPPORTED, "mirrored or periodic side needs 4 interior cells");
     }
-    const size_t bytes = slot_bytes(r->nx, r->ny);
+    const size_t bytes = slot_bytes(r->nx, r->ny, s->precision == EB2_MIXED ? 1 : 0);
     if (s->used + bytes > s->budget) return fail(EB2_EBUSY, "HBM budget exhausted");
     int q = -1;
     for (int k = 0; k < s->nslots; k++)
@@ -462,11 +498,8 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
     Slot& sl = s->slots[q];
     const int rows = r->nx + 2 * GC, cols = r->ny + 2 * GC;
     const size_t n = (size_t)4 * rows * cols * sizeof(double);
-    Grid tg{};
-    tg.nx = r->nx;
-    tg.ny = r->ny;
-    const int ntiles = stage_blocks(tg, s->precision == EB2_MIXED);
-    const int npart = std::max(ntiles, 296);
+    const int prec = s->precision == EB2_MIXED ? 1 : 0;
+    const int npart = slot_partials(r->nx, r->ny, prec);
     // Any failure from here on releases what this call allocated and leaves
     // the slot unused, so that a failed admission leaks nothing.
     auto undo = [&](int code) {
@@ -518,7 +551,7 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
         for (int m = 0; m < 4; m++) sd.bnd.fixed[m][k] = mach3[k];
     }
     sd.tiles_x = (r->ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y;
-    sd.ntiles = ntiles;
+    for (int k = 0; k < s->nshapes; k++) sd.ntiles[k] = slot_tiles(r->nx, r->ny, prec, k);
     sd.ncells = r->nx * r->ny;
     CKU(launch_init(sl.u, sd.grid, sd.gas, d, s->stream));
     // control block and first CFL step, as eb2_run starts a solve

@@ -27,24 +27,32 @@
 namespace eb2 {
 namespace mixstage {
 
-constexpr int TX = MIXED_TILE_X, TY = STAGE_TILE_Y, NT = 256;
-// CTAs of the stage kernel resident per SM (the register budget follows:
-// 65536 / (NT * CTAS) per thread)
+// A tile shape of the stage kernel: TX x TY cells per CTA of NT threads, CTAS
+// CTAs resident per SM (the register budget is 65536 / (NT CTAS) per thread).
+// The solve server's autotuner picks one of the shapes of MixedShapes per
+// batch-shape class; single solves use Shape16.
+template <int TX_, int TY_, int NT_, int CTAS_>
+struct Shape {
+    static constexpr int TX = TX_, TY = TY_, NT = NT_, CTAS = CTAS_;
+    static constexpr int HX = TX + 6, HY = TY + 6;    // conserved tile with halos
+    static constexpr int PX = TX + 2, PY = TY + 2;    // primitives: tile + first ring
+    static constexpr int FS = HX * HY, PS = PX * PY;
+    static constexpr int XS = (TX + 1) * TY, YS = TX * (TY + 1);  // x and y faces
+    static constexpr int NJX = XS, NJY = YS;
+    // FP32 face fluxes (widened exactly where read, so that both cells of a face
+    // see the same value, the flux differences telescope and the step conserves
+    // to FP64 round-off), FP32 tile, FP32 primitives
+    static constexpr size_t SMEM =
+        (size_t)(XS + YS + FS + PS) * sizeof(float4) + (size_t)PS * sizeof(float2);
+    static_assert(TX * TY % NT == 0, "whole cells per thread");
+    static_assert((NJX + NJY + NT - 1) / NT <= 32, "one vacuum bit per job of a thread");
+};
 #ifndef EB2_MIXED_CTAS
 #define EB2_MIXED_CTAS 4
 #endif
-constexpr int CTAS = EB2_MIXED_CTAS;
-constexpr int HX = TX + 6, HY = TY + 6;
-constexpr int PX = TX + 2, PY = TY + 2;
-constexpr int FS = HX * HY;
-constexpr int PS = PX * PY;
-constexpr int XS = (TX + 1) * TY;
-constexpr int YS = TX * (TY + 1);
-constexpr int NJX = (TX + 1) * TY, NJY = TX * (TY + 1);
-// FP32 face fluxes (widened exactly where read, so that both cells of a face
-// see the same value, the flux differences telescope and the step conserves
-// to FP64 round-off), FP32 tile, FP32 primitives
-constexpr size_t SMEM = (size_t)(XS + YS + FS + PS) * sizeof(float4) + (size_t)PS * sizeof(float2);
+using Shape16 = Shape<MIXED_TILE_X, STAGE_TILE_Y, 256, EB2_MIXED_CTAS>;
+using Shape8 = Shape<8, STAGE_TILE_Y, 128, 8>;
+using Shape32 = Shape<32, STAGE_TILE_Y, 512, 2>;
 
 // Conserved differences of both sides of an interface next to a near-vacuum
 // cell: the stencil's six cells are read in FP64 from the stage input (cell i at
@@ -209,8 +217,10 @@ EB2_HD unsigned interface_flux(const float4* __restrict__ s, int stride,
 }
 
 // One tile (ti, tj) of one stage; shared by the single-solve and batched kernels.
-template <bool WZ, int FLUX>
+template <class S, bool WZ, int FLUX>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, int tiles_x) {
+    constexpr int TX = S::TX, TY = S::TY, NT = S::NT, HY = S::HY, PX = S::PX, PY = S::PY;
+    constexpr int FS = S::FS, PS = S::PS, XS = S::XS, YS = S::YS, NJX = S::NJX, NJY = S::NJY;
     Ctrl* ctrl = a.ctrl;
     if (!ctrl->active) return;
     extern __shared__ float4 smv[];
@@ -272,7 +282,6 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     // their own with the FP64 eigenvector matrices.
     unsigned st = 0, vac = 0;
     const int pos = a.num.positivity;
-    static_assert((NJX + NJY + NT - 1) / NT <= 32, "one vacuum bit per job of a thread");
     auto face = [&](auto vacuum, int job) -> unsigned {
         constexpr bool VAC = decltype(vacuum)::value;
         if (job < NJX) {
@@ -316,7 +325,6 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     const double grav = a.num.gravity;
     double mx = 0.0, my = 0.0, ps = 0.0;
     constexpr int NC = TX * TY / NT;
-    static_assert(TX * TY % NT == 0, "whole cells per thread");
     double xs[NC][4], ys[NC][4];
 #pragma unroll
     for (int t = 0; t < NC; t++) {
@@ -414,27 +422,28 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
 }
 
 // Single solve: one CTA per tile.
-template <bool WZ, int FLUX>
-__global__ void __launch_bounds__(NT, CTAS) k_stage(StageArgs a) {
-    stage_tile<WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
+template <class S, bool WZ, int FLUX>
+__global__ void __launch_bounds__(S::NT, S::CTAS) k_stage(StageArgs a) {
+    stage_tile<S, WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 template <bool WZ, int FLUX>
 cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
-    auto kern = k_stage<WZ, FLUX>;
+    using S = Shape16;
+    auto kern = k_stage<S, WZ, FLUX>;
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!configured[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)SMEM);
+                                             (int)S::SMEM);
         if (e != cudaSuccess) return e;
         configured[dev] = true;
     }
     if (!a.uout) return cudaSuccess;
-    dim3 grid((a.grid.ny + TY - 1) / TY, (a.grid.nx + TX - 1) / TX);
-    kern<<<grid, NT, SMEM, s>>>(a);
+    dim3 grid((a.grid.ny + S::TY - 1) / S::TY, (a.grid.nx + S::TX - 1) / S::TX);
+    kern<<<grid, S::NT, S::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
