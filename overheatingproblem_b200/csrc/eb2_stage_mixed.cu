@@ -15,9 +15,13 @@ static cudaError_t by_flux(const StageArgs& a, cudaStream_t s) {
         case FLUX_HLLHC: return mixstage::launch_one<WZ, FLUX_HLLHC>(a, s);
         case FLUX_HLLCHC: return mixstage::launch_one<WZ, FLUX_HLLCHC>(a, s);
         case FLUX_ROEHC: return mixstage::launch_one<WZ, FLUX_ROEHC>(a, s);
-        default: return cudaErrorNotSupported;  // no mixed heat-conduction fluxes
+        default: return cudaErrorNotSupported;
     }
 }
+
+// Tile rows of the single-solve mixed stage (its partials hold one triple per
+// tile).
+int mixed_solve_tile_x() { return mixstage::SolveShape::TX; }
 
 cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s) {
     // the mixed form implements the characteristic WENO5 reconstruction only

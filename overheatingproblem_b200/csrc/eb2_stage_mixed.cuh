@@ -76,6 +76,22 @@ EB2_HD void vacuum_delta(const double* __restrict__ u, size_t g2,
         qa[m] = u[g2 + m * plane];
         qb[m] = u[g2 + step + m * plane];
     }
+    // a stencil of six equal cells (the undisturbed gas ahead of a front) has
+    // zero differences on both sides: nothing to project
+    bool flat = true;
+#pragma unroll
+    for (int m = 0; m < 4; m++) flat = flat && qa[m] == qb[m];
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        if (n == 2 || n == 3) continue;
+#pragma unroll
+        for (int m = 0; m < 4; m++) flat = flat && u[g2 + (n - 2) * step + m * plane] == qa[m];
+    }
+    if (flat) {
+#pragma unroll
+        for (int m = 0; m < 4; m++) dq[m] = f32::f2s(0.0f);
+        return;
+    }
     double A[5], B[5];
     x64::primitive5(qa[0], qa[1], qa[2], qa[3], g, A);
     x64::primitive5(qb[0], qb[1], qb[2], qb[3], g, B);
@@ -427,9 +443,17 @@ __global__ void __launch_bounds__(S::NT, S::CTAS) k_stage(StageArgs a) {
     stage_tile<S, WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
+// Tile shape of single solves (0: Shape16, 1: Shape8, 2: Shape32).
+#ifndef EB2_MIXED_SOLVE_SHAPE
+#define EB2_MIXED_SOLVE_SHAPE 0
+#endif
+using SolveShape = std::conditional_t<EB2_MIXED_SOLVE_SHAPE == 1, Shape8,
+                                      std::conditional_t<EB2_MIXED_SOLVE_SHAPE == 2, Shape32,
+                                                         Shape16>>;
+
 template <bool WZ, int FLUX>
 cudaError_t launch_one(const StageArgs& a, cudaStream_t s) {
-    using S = Shape16;
+    using S = SolveShape;
     auto kern = k_stage<S, WZ, FLUX>;
     static bool configured[64] = {};
     int dev = 0;
