@@ -128,6 +128,8 @@ struct eb2_server {
     int bc_grid = 8;                         // blocks of the ghost-fill launches
     int active_grid = 8;                     // blocks of the end-of-step launches
     long long graph_launches = 0;
+    cudaEvent_t busy0 = nullptr, busy1 = nullptr;  // around each eb2_server_step's graphs
+    double busy_ms = 0.0;                    // their accumulated device time
 };
 
 namespace {
@@ -444,6 +446,8 @@ int eb2_server_destroy(eb2_server* s) {
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     destroy_graphs(s);
+    if (s->busy0) cudaEventDestroy(s->busy0);
+    if (s->busy1) cudaEventDestroy(s->busy1);
     for (auto& sl : s->slots)
         if (sl.used) {
             cudaFree(sl.u);
@@ -583,9 +587,25 @@ int eb2_server_step(eb2_server* s, int ngraphs, int* nfinished) {
         if (int r = rebuild(s)) return r;
     if (nfinished) *nfinished = 0;
     if (s->nwork == 0) return EB2_OK;
+    if (!s->busy0) {
+        CKS(cudaEventCreate(&s->busy0));
+        CKS(cudaEventCreate(&s->busy1));
+    }
+    CKS(cudaEventRecord(s->busy0, s->stream));
     for (int k = 0; k < ngraphs; k++)
         if (int r = launch_steps(s)) return r;
-    return harvest(s, nfinished);
+    CKS(cudaEventRecord(s->busy1, s->stream));
+    int r = harvest(s, nfinished);  // synchronizes the stream
+    float ms = 0.0f;
+    if (!r && cudaEventElapsedTime(&ms, s->busy0, s->busy1) == cudaSuccess) s->busy_ms += ms;
+    return r;
+}
+
+// Device time of the batch steps so far (the graphs of every eb2_server_step).
+int eb2_server_busy_time(eb2_server* s, double* busy_ms) {
+    if (!s || !busy_ms) return fail(EB2_EARG, "null argument");
+    *busy_ms = s->busy_ms;
+    return EB2_OK;
 }
 
 int eb2_server_poll(eb2_server* s, long long* ids, double* t_final, long long* steps,

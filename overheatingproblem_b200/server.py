@@ -100,6 +100,12 @@ class Server:
         L.check(self._lib.eb2_server_fetch(self._h, rid, None if out is None else L.dptr(out)))
         return out
 
+    def busy_ms(self) -> float:
+        """Device time of the batch steps so far (ms)."""
+        ms = C.c_double()
+        L.check(self._lib.eb2_server_busy_time(self._h, C.byref(ms)))
+        return ms.value
+
     def stats(self):
         used, act, gl = C.c_ulonglong(), C.c_int(), C.c_longlong()
         L.check(self._lib.eb2_server_stats(self._h, C.byref(used), C.byref(act), C.byref(gl)))
