@@ -125,6 +125,7 @@ struct eb2_server {
     int sms = 148;
     std::map<int, cudaGraphExec_t> graphs;   // launch key (grid_key) -> graph
     std::map<int, int> tuned;                // batch-shape class -> launch key
+    std::map<int, float> tuned_ms;           // batch-shape class -> its graph's time
     int bc_grid = 8;                         // blocks of the ghost-fill launches
     int active_grid = 8;                     // blocks of the end-of-step launches
     long long graph_launches = 0;
@@ -338,6 +339,7 @@ int launch_steps(eb2_server* s) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         s->tuned[cls] = best;
+        s->tuned_ms[cls] = best_ms;
         return use_shape(s, best >> 24);
     }
     if (int r = use_shape(s, it->second >> 24)) return r;
@@ -700,7 +702,14 @@ int eb2_server_run_trace(eb2_server* s, const eb2_request* reqs, const double* a
             continue;
         }
         int nf = 0;
-        if (int rc = eb2_server_step(s, 1, &nf)) return rc;
+        // enough graphs per call that the GPU works ~2 ms between the host's
+        // harvests (a small batch's graph takes a fraction of that, and the
+        // host's admission and retirement work would otherwise leave it idle)
+        int ngraphs = 1;
+        auto tm = s->tuned_ms.find(shape_class(s->nwork0));
+        if (!s->dirty && tm != s->tuned_ms.end() && tm->second > 0.0f)
+            ngraphs = std::max(1, std::min(16, (int)(2.0f / tm->second)));
+        if (int rc = eb2_server_step(s, ngraphs, &nf)) return rc;
         if (!nf) continue;
         const double tf = now_s() - t0;
         for (int q = 0; q < s->nslots; q++) {
