@@ -168,14 +168,17 @@ def serve_stream(eb2, local, n, rate, seed, reps=1, nsample=16):
     with Server(device=local, precision=eb2.lib.MIXED, scheme=2,
                 hbm_budget=120 * 10**9) as srv:
         for _ in range(reps):
-            b0 = srv.busy_ms()
+            t0 = srv.timing()
             runs.append(srv.run_trace(reqs, arr, keep_results=sample))
-            runs[-1]["busy_s"] = (srv.busy_ms() - b0) * 1e-3
+            t1 = srv.timing()
+            runs[-1]["timing"] = {k: t1[k] - t0[k] for k in t1}
     order = sorted(range(reps), key=lambda k: runs[k]["makespan"])
     out = runs[order[len(order) // 2]]
     batched = arm_summary(n, out["makespan"], out["finish"] - arr, out["status"])
     batched["steps"] = int(out["steps"].sum())
-    batched["gpu_busy_frac"] = out["busy_s"] / out["makespan"]
+    batched["gpu_busy_frac"] = out["timing"]["busy_s"] / out["makespan"]
+    batched["host_autotune_s"] = out["timing"]["tune_s"]
+    batched["host_admin_s"] = out["timing"]["admin_s"]
     batched["replays_solves_per_s"] = [n / o["makespan"] for o in runs]
     fin_m, st_m, _ = one_at_a_time(eb2, local, reqs, arr, eb2.lib.MIXED, set())
     mixed1 = arm_summary(n, fin_m[-1], fin_m - arr, st_m)

@@ -278,9 +278,11 @@ int eb2_server_poll(eb2_server *srv, long long *ids, double *t_final, long long 
 /* Copy a finished solve's state to U (may be NULL) and free its slot. */
 int eb2_server_fetch(eb2_server *srv, long long id, double *U);
 /* Device time of every batch step run so far (CUDA events around the graphs
- * of each eb2_server_step): set against a replay's wall time it is the share
- * of the time the GPU spent stepping solves. */
-int eb2_server_busy_time(eb2_server *srv, double *busy_ms);
+ * of each eb2_server_step; set against a replay's wall time it is the share of
+ * the time the GPU spent stepping solves), and the host seconds spent in the
+ * autotuner's trials and in admission, work-list rebuilds and retirement.
+ * Any output pointer may be NULL. */
+int eb2_server_timing(eb2_server *srv, double *busy_ms, double *tune_s, double *admin_s);
 int eb2_server_stats(eb2_server *srv, unsigned long long *hbm_used, int *active,
                      long long *graph_launches);
 /* The request loop: replay n requests arriving arrival_s[i] seconds after the

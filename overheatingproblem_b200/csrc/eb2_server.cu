@@ -131,7 +131,19 @@ struct eb2_server {
     long long graph_launches = 0;
     cudaEvent_t busy0 = nullptr, busy1 = nullptr;  // around each eb2_server_step's graphs
     double busy_ms = 0.0;                    // their accumulated device time
+    double tune_s = 0.0;                     // host time in autotuner trials
+    double admin_s = 0.0;                    // host time in admission, rebuilds, retirement
 };
+
+namespace {
+// Adds the wall time of a scope to a server counter.
+struct HostTimer {
+    double& acc;
+    double t0;
+    explicit HostTimer(double& a) : acc(a), t0(now_s()) {}
+    ~HostTimer() { acc += now_s() - t0; }
+};
+}  // namespace
 
 namespace {
 
@@ -189,6 +201,7 @@ int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
 
 // Rewrite the work list and descriptors after admissions and retirements.
 int rebuild(eb2_server* s) {
+    HostTimer timer(s->admin_s);
     int n = 0, n0 = 0;
     for (int q = 0; q < s->nslots; q++)
         if (s->slots[q].used && !s->slots[q].done) {
@@ -298,6 +311,7 @@ int launch_steps(eb2_server* s) {
     const int cls = shape_class(s->nwork0);
     auto it = s->tuned.find(cls);
     if (it == s->tuned.end()) {
+        HostTimer timer(s->tune_s);
         // the slots advance during the trials, which is ordinary progress
         int best = 0;
         float best_ms = 1e30f;
@@ -478,6 +492,7 @@ int eb2_server_destroy(eb2_server* s) {
 
 int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
     if (!s || !r) return fail(EB2_EARG, "null argument");
+    HostTimer timer(s->admin_s);
     if (r->nx < 1 || r->ny < 1) return fail(EB2_EARG, "empty grid");
     CKS(cudaSetDevice(s->device));
     InitDesc d;
@@ -603,10 +618,14 @@ int eb2_server_step(eb2_server* s, int ngraphs, int* nfinished) {
     return r;
 }
 
-// Device time of the batch steps so far (the graphs of every eb2_server_step).
-int eb2_server_busy_time(eb2_server* s, double* busy_ms) {
-    if (!s || !busy_ms) return fail(EB2_EARG, "null argument");
-    *busy_ms = s->busy_ms;
+// Device time of the batch steps so far (the graphs of every eb2_server_step),
+// and the host time spent in autotuner trials and in admission, rebuilds and
+// retirement.
+int eb2_server_timing(eb2_server* s, double* busy_ms, double* tune_s, double* admin_s) {
+    if (!s) return fail(EB2_EARG, "null server");
+    if (busy_ms) *busy_ms = s->busy_ms;
+    if (tune_s) *tune_s = s->tune_s;
+    if (admin_s) *admin_s = s->admin_s;
     return EB2_OK;
 }
 
@@ -629,6 +648,7 @@ int eb2_server_poll(eb2_server* s, long long* ids, double* t_final, long long* s
 
 int eb2_server_fetch(eb2_server* s, long long id, double* U) {
     if (!s) return fail(EB2_EARG, "null server");
+    HostTimer timer(s->admin_s);
     CKS(cudaSetDevice(s->device));
     int q = find_slot(s, id);
     if (q < 0) return fail(EB2_EARG, "unknown request id %lld", id);

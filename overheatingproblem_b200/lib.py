@@ -113,7 +113,8 @@ SIGNATURES = {
     "eb2_server_destroy": (C.c_int, [_vp]),
     "eb2_server_submit": (C.c_int, [_vp, C.POINTER(Request), C.POINTER(C.c_longlong)]),
     "eb2_server_step": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
-    "eb2_server_busy_time": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "eb2_server_timing": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)]),
     "eb2_server_poll": (C.c_int, [_vp, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_longlong),
                                   C.POINTER(C.c_uint), C.c_int, C.POINTER(C.c_int)]),
     "eb2_server_fetch": (C.c_int, [_vp, C.c_longlong, _dp]),

@@ -100,11 +100,13 @@ class Server:
         L.check(self._lib.eb2_server_fetch(self._h, rid, None if out is None else L.dptr(out)))
         return out
 
-    def busy_ms(self) -> float:
-        """Device time of the batch steps so far (ms)."""
-        ms = C.c_double()
-        L.check(self._lib.eb2_server_busy_time(self._h, C.byref(ms)))
-        return ms.value
+    def timing(self) -> dict:
+        """Device time of the batch steps so far (s), and the host seconds in
+        autotuner trials and in admission, rebuilds and retirement."""
+        ms, tune, admin = C.c_double(), C.c_double(), C.c_double()
+        L.check(self._lib.eb2_server_timing(self._h, C.byref(ms), C.byref(tune),
+                                            C.byref(admin)))
+        return {"busy_s": ms.value * 1e-3, "tune_s": tune.value, "admin_s": admin.value}
 
     def stats(self):
         used, act, gl = C.c_ulonglong(), C.c_int(), C.c_longlong()
