@@ -94,6 +94,11 @@ double now_s() {
 struct eb2_server {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // The server's own stream-ordered memory pool: slot buffers and work lists
+    // come from it, and memory a retired slot frees stays reserved in it (up
+    // to the HBM budget) for the next admission instead of being unmapped and
+    // mapped again.
+    cudaMemPool_t pool = nullptr;
     int precision = EB2_MIXED;
     Numerics num{};
     double gamma = 1.4;
@@ -216,7 +221,7 @@ int rebuild(eb2_server* s) {
             CKS(cudaStreamSynchronize(s->stream));
             cudaFreeHost(s->h_work);
         }
-        CKS(cudaMallocAsync(&s->d_work, (size_t)cap * sizeof(int2), s->stream));
+        CKS(cudaMallocFromPoolAsync(&s->d_work, (size_t)cap * sizeof(int2), s->pool, s->stream));
         CKS(cudaMallocHost(&s->h_work, (size_t)cap * sizeof(int2)));
         s->work_cap = cap;
         destroy_graphs(s);  // graphs hold the old work-list address
@@ -239,7 +244,8 @@ int rebuild(eb2_server* s) {
             CKS(cudaStreamSynchronize(s->stream));
             cudaFreeHost(s->h_bcwork);
         }
-        CKS(cudaMallocAsync(&s->d_bcwork, (size_t)cap * sizeof(int2), s->stream));
+        CKS(cudaMallocFromPoolAsync(&s->d_bcwork, (size_t)cap * sizeof(int2), s->pool,
+                                    s->stream));
         CKS(cudaMallocHost(&s->h_bcwork, (size_t)cap * sizeof(int2)));
         s->bc_cap = cap;
         destroy_graphs(s);  // graphs hold the old list address
@@ -325,9 +331,12 @@ int launch_steps(eb2_server* s) {
             // the tiles of shape 0, a 32-row one at most as many)
             const int each_grid = 1 << (cls + (batch_shape_tile_x(prec, sh) <
                                                batch_shape_tile_x(prec, 0) ? 1 : 0));
+            // persistent grids are tried in the default shape only: the trials
+            // cost host time (a capture each) and progress at a worse rate
             std::vector<int> keys;
-            for (int mult = 1; mult <= stage_batch_max_blocks_per_sm(prec, sh); mult++)
-                if (mult * s->sms < s->nwork) keys.push_back(grid_key(sh, mult * s->sms, 0));
+            if (sh == 0)
+                for (int mult = 1; mult <= stage_batch_max_blocks_per_sm(prec, sh); mult++)
+                    if (mult * s->sms < s->nwork) keys.push_back(grid_key(sh, mult * s->sms, 0));
             keys.push_back(grid_key(sh, each_grid, 1));
             for (int key : keys) {
                 cudaGraphExec_t ex;
@@ -436,6 +445,14 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
         eb2_server_destroy(s);
         return code;
     };
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    unsigned long long keep = hbm_budget_bytes;
+    if (cudaMemPoolCreate(&s->pool, &props) ||
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep))
+        return bail(fail(EB2_ECUDA, "server memory pool"));
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) ||
         cudaMalloc(&s->d_desc, (size_t)max_slots * sizeof(SlotDesc)) ||
         cudaMallocHost(&s->h_desc, (size_t)max_slots * sizeof(SlotDesc)) ||
@@ -486,6 +503,7 @@ int eb2_server_destroy(eb2_server* s) {
     cudaFree(s->d_active);
     cudaFreeHost(s->h_active);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return EB2_OK;
 }
@@ -541,10 +559,11 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
         if (e_ != cudaSuccess)                                                           \
             return undo(fail(EB2_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_)));       \
     } while (0)
-    CKU(cudaMallocAsync(&sl.u, n, s->stream));
-    CKU(cudaMallocAsync(&sl.u1, n, s->stream));
-    CKU(cudaMallocAsync(&sl.u2, n, s->stream));
-    CKU(cudaMallocAsync(&sl.partials, (size_t)3 * npart * sizeof(double), s->stream));
+    CKU(cudaMallocFromPoolAsync(&sl.u, n, s->pool, s->stream));
+    CKU(cudaMallocFromPoolAsync(&sl.u1, n, s->pool, s->stream));
+    CKU(cudaMallocFromPoolAsync(&sl.u2, n, s->pool, s->stream));
+    CKU(cudaMallocFromPoolAsync(&sl.partials, (size_t)3 * npart * sizeof(double), s->pool,
+                                s->stream));
     CKU(cudaMemsetAsync(sl.u, 0, n, s->stream));
     CKU(cudaMemsetAsync(sl.u1, 0, n, s->stream));
     CKU(cudaMemsetAsync(sl.u2, 0, n, s->stream));
