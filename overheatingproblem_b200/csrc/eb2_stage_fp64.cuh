@@ -192,27 +192,30 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
         __syncthreads();
     }
 
-    // 3. interface fluxes: x faces (TX+1) x TY, then y faces TX x (TY+1).
+    // 3. interface fluxes: x faces (TX+1) x TY in one loop, then y faces
+    // TX x (TY+1) in another, so that each loop carries one direction's code and
+    // live state (with 15 x 32 tiles each takes two passes of the 256 threads).
     // A face whose WENO operands leave the range of the branch-free divisions
     // is marked in `redo` (bit = this thread's job number) and recomputed with
     // `/` after the pass, so the common pass carries no fallback code.
     unsigned st = 0;
     const int pos = a.num.positivity;
     unsigned redo = 0;
-    static_assert((NJX + NJY + NT - 1) / NT <= 32, "one redo bit per job of a thread");
+    constexpr int PXF = (NJX + NT - 1) / NT, PYF = (NJY + NT - 1) / NT;
+    static_assert(PXF + PYF <= 32, "one redo bit per job of a thread");
     // (faces that no interior cell of this tile uses -- past the domain edge in
     // a partial tile -- are skipped)
-    auto face = [&](auto rn, int job) -> unsigned {
+    auto xface = [&](auto rn, int job) -> unsigned {
         constexpr bool RN = decltype(rn)::value;
-        if (job < NJX) {
-            int rr = job / TY, cc = job - rr * TY;
-            if (i0 - 1 + rr >= rows - GC || j0 + cc >= cols - GC) return 0u;
-            const double* s = sU + rr * HY + (cc + 3);
-            const double* pa = sP + rr * PY + (cc + 1);
-            return interface_flux<RN, 1, RECON, CHAR, WZ, FLUX>(s, HY, pa, pa + PY, a.grid.dx, g,
-                                                                pos, sFx + rr * TY + cc, XS);
-        }
-        int q = job - NJX;
+        int rr = job / TY, cc = job - rr * TY;
+        if (i0 - 1 + rr >= rows - GC || j0 + cc >= cols - GC) return 0u;
+        const double* s = sU + rr * HY + (cc + 3);
+        const double* pa = sP + rr * PY + (cc + 1);
+        return interface_flux<RN, 1, RECON, CHAR, WZ, FLUX>(s, HY, pa, pa + PY, a.grid.dx, g,
+                                                            pos, sFx + rr * TY + cc, XS);
+    };
+    auto yface = [&](auto rn, int q) -> unsigned {
+        constexpr bool RN = decltype(rn)::value;
         int rr = q / (TY + 1), cc = q - rr * (TY + 1);
         if (i0 + rr >= rows - GC || j0 - 1 + cc >= cols - GC) return 0u;
         const double* s = sU + (rr + 3) * HY + cc;
@@ -220,14 +223,21 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
         return interface_flux<RN, 2, RECON, CHAR, WZ, FLUX>(s, 1, pa, pa + 1, a.grid.dy, g, pos,
                                                             sFy + rr * (TY + 1) + cc, YS);
     };
-    for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++) {
-        const unsigned r = face(std::true_type{}, job);
+    for (int job = threadIdx.x, n = 0; job < NJX; job += NT, n++) {
+        const unsigned r = xface(std::true_type{}, job);
+        if (r & ST_REDO) redo |= 1u << n;
+        else st |= r;
+    }
+    for (int q = threadIdx.x, n = PXF; q < NJY; q += NT, n++) {
+        const unsigned r = yface(std::true_type{}, q);
         if (r & ST_REDO) redo |= 1u << n;
         else st |= r;
     }
     if (__syncthreads_or(redo != 0u)) {
-        for (int job = threadIdx.x, n = 0; job < NJX + NJY; job += NT, n++)
-            if (redo >> n & 1u) st |= face(std::false_type{}, job);
+        for (int job = threadIdx.x, n = 0; job < NJX; job += NT, n++)
+            if (redo >> n & 1u) st |= xface(std::false_type{}, job);
+        for (int q = threadIdx.x, n = PXF; q < NJY; q += NT, n++)
+            if (redo >> n & 1u) st |= yface(std::false_type{}, q);
         __syncthreads();
     }
 
