@@ -312,9 +312,9 @@ def short_accuracy(acc):
             "last_t_with_l1_rho_le_1e-6": acc["last_t_with_l1_rho_le_1e-6"]}
 
 
-def run_extras(eb2, local, peak, rate, nserve):
-    """Whole runs, mid-run windows, accuracy and the served stream (one GPU)."""
-    extra, acc = {}, {}
+def run_extras(eb2, local, peak, rate, nserve, extra, acc):
+    """Whole runs, mid-run windows, accuracy and the served stream (one GPU),
+    filled into `extra` and `acc` as each is measured."""
     # 1024^2: FP64 and mixed whole runs (HLLC, Roe), the FP32-sized floor
     for name, sch in (("hllc", 2), ("roe", 3)):
         s64, dx, dy, i64, r64, f64, _ = whole_run(eb2, local, 1024, "fp64", sch)
@@ -359,7 +359,6 @@ def run_extras(eb2, local, peak, rate, nserve):
     del r64, f64
     if nserve:
         extra["served_stream"] = serve_stream(eb2, local, nserve, rate, 7)
-    return extra, acc
 
 
 def run_accuracy(args, local):
@@ -788,15 +787,13 @@ def run_ours(args, world, rank, local):
                "path": "eb2_upload + eb2_delta_t + eb2_rk_step + eb2_download"}
     s.close()
 
-    extra, accuracy = {}, None
-    if not args.no_extra and world == 1:
-        extra, accuracy = run_extras(eb2, local, peak, args.serve_rate, args.serve_requests)
-
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, per_step, n, kind, cores = cpu_rate(nx, scheme, 20.0, 40, 3)
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": kind,
                "sample": f"{n} full SSP-RK3 steps of the {nx}^2 grid ({per_step:.3f} s each)"}
+    extra, accuracy = {}, {}
+    line = None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -808,7 +805,22 @@ def run_ours(args, world, rank, local):
             "step_ms_min_median_max": [min(step_ms), float(np.median(step_ms)), max(step_ms)],
             "extra": extra,
         }
-        if accuracy is not None:
+    if line is not None and not args.no_extra and world == 1:
+        # The extras take minutes.  If the run is stopped by SIGTERM meanwhile,
+        # the line is printed with the extras measured so far.
+        import signal
+
+        def stop(signum, frame):
+            line["extra_incomplete"] = "stopped by signal %d during the extras" % signum
+            if accuracy:
+                line["accuracy"] = accuracy
+            print(json.dumps(line), flush=True)
+            os._exit(0)
+        signal.signal(signal.SIGTERM, stop)
+        run_extras(eb2, local, peak, args.serve_rate, args.serve_requests, extra, accuracy)
+        signal.signal(signal.SIGTERM, signal.SIG_DFL)
+    if line is not None:
+        if accuracy:
             line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
 
