@@ -32,18 +32,21 @@ struct SlotDesc {
     int tiles_x;          // tiles along y (32 columns in every shape)
     int ntiles[kMixedShapes];  // tiles of the slot in each tile shape
     int ncells;
+    int npartials;        // CFL partial triples its stage kernels write (mixed: per
+                          // 8 x 32 block in every tile shape; FP64: per tile)
     int bc_blocks;        // ghost-fill blocks of this slot (its entries in the bc work list)
 };
 
 // Stage buffers of SSP-RK3 (the server runs third-order steps only).
-__device__ __forceinline__ void rk3_buffers(const SlotDesc& s, int stage, const double*& in,
+__host__ __device__ __forceinline__ void rk3_buffers(const SlotDesc& s, int stage, const double*& in,
                                             double*& out, int& comb) {
     if (stage == 0) { in = s.u; out = s.u1; comb = COMB_EULER; }
     else if (stage == 1) { in = s.u1; out = s.u2; comb = COMB_RK3_2; }
     else { in = s.u2; out = s.u; comb = COMB_RK3_3; }
 }
 
-__device__ __forceinline__ StageArgs slot_args(const SlotDesc& s, int stage) {
+// (on the host too: the stage arguments of a slot with a launch of its own)
+__host__ __device__ __forceinline__ StageArgs slot_args(const SlotDesc& s, int stage) {
     StageArgs a;
     rk3_buffers(s, stage, a.uin, a.uout, a.combine);
     a.un = s.u;
@@ -79,6 +82,11 @@ cudaError_t launch_stage_batch_fp64(const BatchLaunch& b, const Numerics& num, i
                                     cudaStream_t s);
 cudaError_t launch_stage_batch_mixed(const BatchLaunch& b, const Numerics& num, int stage,
                                      cudaStream_t s);
+// One stage of one slot as a launch of its own (the single-solve grid of tiles
+// in batched tile shape `shape`, the arguments in the kernel's parameter
+// block): the server gives this to slots that fill the GPU by themselves.
+cudaError_t launch_stage_slot_mixed(const StageArgs& a, const Numerics& num, int shape,
+                                    cudaStream_t s);
 cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s);
 cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s);
 // Tile shapes of a server's stage kernels (1 for FP64, kMixedShapes for the

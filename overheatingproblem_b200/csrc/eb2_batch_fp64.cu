@@ -110,16 +110,16 @@ cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s) {
 
 // End of a step for every active slot: one block per slot.
 __global__ void k_finalize_batch(const SlotDesc* __restrict__ slots, const int* __restrict__ act,
-                                 const int* __restrict__ nact, int shape) {
+                                 const int* __restrict__ nact) {
     __shared__ double red[96];
     if ((int)blockIdx.x >= *nact) return;
     const SlotDesc& sd = slots[act[blockIdx.x]];
     if (!sd.ctrl) return;
-    finalize_body(sd.ctrl, sd.partials, sd.ntiles[shape], sd.ncells, 2, red);
+    finalize_body(sd.ctrl, sd.partials, sd.npartials, sd.ncells, 2, red);
 }
 
 cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s) {
-    k_finalize_batch<<<b.active_grid, 256, 0, s>>>(b.slots, b.active, b.nactive, b.shape);
+    k_finalize_batch<<<b.active_grid, 256, 0, s>>>(b.slots, b.active, b.nactive);
     return cudaGetLastError();
 }
 

@@ -10,6 +10,21 @@ cudaError_t launch_stage_batch_mixed_s8(const BatchLaunch& b, const Numerics& nu
 cudaError_t launch_stage_batch_mixed_s32(const BatchLaunch& b, const Numerics& num, int stage,
                                          cudaStream_t s);
 
+cudaError_t launch_stage_slot_mixed_s8(const StageArgs& a, const Numerics& num,
+                                       cudaStream_t s);
+cudaError_t launch_stage_slot_mixed_s32(const StageArgs& a, const Numerics& num,
+                                        cudaStream_t s);
+
+cudaError_t launch_stage_slot_mixed(const StageArgs& a, const Numerics& num, int shape,
+                                    cudaStream_t s) {
+    switch (shape) {
+        case 0: return batchmixed::launch_slot<mixstage::Shape16>(a, num, s);
+        case 1: return launch_stage_slot_mixed_s8(a, num, s);
+        case 2: return launch_stage_slot_mixed_s32(a, num, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_stage_batch_mixed(const BatchLaunch& b, const Numerics& num, int stage,
                                      cudaStream_t s) {
     switch (b.shape) {

@@ -47,6 +47,52 @@ __global__ void __launch_bounds__(S::NT, S::CTAS)
     mixstage::stage_tile<S, WZ, FLUX>(sa, tile.x, tile.y, tile.z);
 }
 
+// One slot's stage as a launch of its own: a CTA per tile, as the
+// single-solve kernel, with the stage arguments in the parameter block.
+template <class S, bool WZ, int FLUX>
+__global__ void __launch_bounds__(S::NT, S::CTAS) k_stage_slot_mixed(StageArgs a) {
+    mixstage::stage_tile<S, WZ, FLUX>(a, blockIdx.y, blockIdx.x, gridDim.x);
+}
+
+template <class S, bool WZ, int FLUX>
+cudaError_t one_slot(const StageArgs& a, cudaStream_t s) {
+    auto kern = k_stage_slot_mixed<S, WZ, FLUX>;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)S::SMEM);
+        if (e != cudaSuccess) return e;
+        configured[dev] = true;
+    }
+    if (!a.uout) return cudaSuccess;  // configuration only
+    dim3 grid((a.grid.ny + S::TY - 1) / S::TY, (a.grid.nx + S::TX - 1) / S::TX);
+    kern<<<grid, S::NT, S::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, bool WZ>
+cudaError_t slot_by_flux(const StageArgs& a, int flux, cudaStream_t s) {
+    switch (flux) {
+        case FLUX_HLL: return one_slot<S, WZ, FLUX_HLL>(a, s);
+        case FLUX_HLLC: return one_slot<S, WZ, FLUX_HLLC>(a, s);
+        case FLUX_ROE: return one_slot<S, WZ, FLUX_ROE>(a, s);
+        case FLUX_HLLHC: return one_slot<S, WZ, FLUX_HLLHC>(a, s);
+        case FLUX_HLLCHC: return one_slot<S, WZ, FLUX_HLLCHC>(a, s);
+        case FLUX_ROEHC: return one_slot<S, WZ, FLUX_ROEHC>(a, s);
+        default: return one_slot<S, WZ, FLUX_LLF>(a, s);
+    }
+}
+
+template <class S>
+cudaError_t launch_slot(const StageArgs& a, const Numerics& num, cudaStream_t s) {
+    if (num.recon != 5 || !num.characteristic) return cudaErrorNotSupported;
+    return num.weno_z ? slot_by_flux<S, true>(a, num.flux, s)
+                      : slot_by_flux<S, false>(a, num.flux, s);
+}
+
 template <class S, bool WZ, int FLUX>
 cudaError_t one(const BatchLaunch& b, int stage, cudaStream_t s) {
     auto kern = k_stage_batch_mixed<S, WZ, FLUX>;

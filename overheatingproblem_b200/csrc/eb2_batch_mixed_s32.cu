@@ -9,4 +9,9 @@ cudaError_t launch_stage_batch_mixed_s32(const BatchLaunch& b, const Numerics& n
     return batchmixed::launch<mixstage::Shape32>(b, num, stage, s);
 }
 
+cudaError_t launch_stage_slot_mixed_s32(const StageArgs& a, const Numerics& num,
+                                       cudaStream_t s) {
+    return batchmixed::launch_slot<mixstage::Shape32>(a, num, s);
+}
+
 }  // namespace eb2

@@ -9,4 +9,9 @@ cudaError_t launch_stage_batch_mixed_s8(const BatchLaunch& b, const Numerics& nu
     return batchmixed::launch<mixstage::Shape8>(b, num, stage, s);
 }
 
+cudaError_t launch_stage_slot_mixed_s8(const StageArgs& a, const Numerics& num,
+                                       cudaStream_t s) {
+    return batchmixed::launch_slot<mixstage::Shape8>(a, num, s);
+}
+
 }  // namespace eb2

@@ -38,6 +38,9 @@ cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s);
 // that its 16 x 32 x faces and 15 x 33 y faces (1007) fill four passes of
 // 256 threads; mixed form: 16 x 32.
 constexpr int FP64_TILE_X = 15, MIXED_TILE_X = 16, STAGE_TILE_Y = 32;
+// The mixed stage kernels write one CFL partial triple per 8-row x 32-column
+// block, whatever their tile shape (each tile shape's rows are a multiple of 8).
+constexpr int MIXED_PARTIAL_ROWS = 8;
 // Blocks of one stage launch of the given form, and the most of either form
 // (the size of a partials buffer).
 int stage_blocks(const Grid& g, bool mixed);

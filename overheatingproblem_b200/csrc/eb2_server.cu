@@ -115,7 +115,7 @@ struct eb2_server {
     int* h_nwork = nullptr;       // pinned
     int work_cap = 0;
     int nwork = 0;                // work-list length in the current tile shape
-    int nwork0 = 0;               // the same in shape 0 (the batch-shape class)
+    int nbatch0 = 0;              // the same in shape 0, for the batch-shape class
     int shape = 0;                // tile shape the work list is built for
     int nshapes = 1;
     int2* d_bcwork = nullptr;     // ghost-fill work list: (slot, block of the slot)
@@ -130,7 +130,6 @@ struct eb2_server {
     int sms = 148;
     std::map<int, cudaGraphExec_t> graphs;   // launch key (grid_key) -> graph
     std::map<int, int> tuned;                // batch-shape class -> launch key
-    std::map<int, float> tuned_ms;           // batch-shape class -> its graph's time
     int bc_grid = 8;                         // blocks of the ghost-fill launches
     int active_grid = 8;                     // blocks of the end-of-step launches
     long long graph_launches = 0;
@@ -138,6 +137,19 @@ struct eb2_server {
     double busy_ms = 0.0;                    // their accumulated device time
     double tune_s = 0.0;                     // host time in autotuner trials
     double admin_s = 0.0;                    // host time in admission, rebuilds, retirement
+    float last_graph_ms = 0.0f;              // device time per graph of the last step call
+    // Slots that fill the GPU by themselves (a mixed slot with at least as many
+    // tiles as the GPU holds CTAs of the default shape) get a stage launch of
+    // their own in the graphs, beside the batched launch of the other slots:
+    // their stage arguments then sit in the kernel's parameter block instead
+    // of being copied to shared memory per CTA.  They stay in the ghost-fill
+    // and end-of-step lists.
+    std::vector<int> own;                    // their slot indices
+    std::vector<long long> own_ids;          // and request ids (a slot index is reused)
+    static constexpr int kSide = 4;          // streams their launches fork onto
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kSide] = {};
 };
 
 namespace {
@@ -178,15 +190,31 @@ int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
                   s->d_active, s->d_counts + 1, s->active_grid};
     b.shape = key >> 24;
     CKS(stage_batch(s, b, 0));  // kernel attributes, outside the capture
+    if (!s->own.empty()) {
+        StageArgs cfg = slot_args(s->h_desc[s->own[0]], 0);
+        cfg.uout = nullptr;  // configuration only
+        CKS(launch_stage_slot_mixed(cfg, s->num, b.shape, s->stream));
+    }
     b.grid = (key & 0xffffff) / 2;
     b.each = key % 2;
     cudaGraph_t g = nullptr;
     CKS(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
+    const int nside = std::min<int>((int)s->own.size(), eb2_server::kSide);
     for (int k = 0; k < kStepsPerGraph && !e; k++) {
         for (int st = 0; st < 3 && !e; st++) {
             e = launch_bc_batch(b, st, s->stream);
+            // the slots with launches of their own run beside the batched launch
+            if (!e && nside) e = cudaEventRecord(s->fork, s->stream);
+            for (int j = 0; j < nside && !e; j++) e = cudaStreamWaitEvent(s->side[j], s->fork, 0);
+            for (size_t q = 0; q < s->own.size() && !e; q++)
+                e = launch_stage_slot_mixed(slot_args(s->h_desc[s->own[q]], st), s->num,
+                                            b.shape, s->side[q % eb2_server::kSide]);
             if (!e) e = stage_batch(s, b, st);
+            for (int j = 0; j < nside && !e; j++) {
+                e = cudaEventRecord(s->join[j], s->side[j]);
+                if (!e) e = cudaStreamWaitEvent(s->stream, s->join[j], 0);
+            }
         }
         if (!e) e = launch_finalize_batch(b, s->stream);
     }
@@ -207,13 +235,28 @@ int get_graph(eb2_server* s, int key, cudaGraphExec_t* out) {
 // Rewrite the work list and descriptors after admissions and retirements.
 int rebuild(eb2_server* s) {
     HostTimer timer(s->admin_s);
-    int n = 0, n0 = 0;
+    std::vector<int> own;
+    std::vector<long long> own_ids;
+    const int fills = s->sms * stage_batch_max_blocks_per_sm(1, 0);
+    int n = 0, nb0 = 0;
     for (int q = 0; q < s->nslots; q++)
         if (s->slots[q].used && !s->slots[q].done) {
-            n += s->h_desc[q].ntiles[s->shape];
-            n0 += s->h_desc[q].ntiles[0];
+            if (s->precision == EB2_MIXED && s->h_desc[q].ntiles[0] >= fills) {
+                own.push_back(q);
+                own_ids.push_back(s->slots[q].id);
+            } else {
+                n += s->h_desc[q].ntiles[s->shape];
+                nb0 += s->h_desc[q].ntiles[0];
+            }
         }
-    s->nwork0 = n0;
+    s->nbatch0 = nb0;
+    if (own_ids != s->own_ids) {
+        // the graphs hold the own launches' arguments, buffer addresses included:
+        // a new request in a reused slot index has buffers of its own
+        s->own = own;
+        s->own_ids = own_ids;
+        destroy_graphs(s);
+    }
     if (n > s->work_cap) {
         int cap = std::max(n, 2 * s->work_cap);
         if (s->d_work) CKS(cudaFreeAsync(s->d_work, s->stream));
@@ -267,6 +310,7 @@ int rebuild(eb2_server* s) {
     int w = 0;
     for (int q = 0; q < s->nslots; q++) {
         if (!s->slots[q].used || s->slots[q].done) continue;
+        if (std::find(s->own.begin(), s->own.end(), q) != s->own.end()) continue;
         for (int t = 0; t < s->h_desc[q].ntiles[s->shape]; t++) s->h_work[w++] = make_int2(q, t);
     }
     *s->h_nwork = w;
@@ -300,6 +344,10 @@ int shape_class(int nwork) {
     return c;
 }
 
+// The batch-shape class the autotuner keys on: log2 of the batched work-list
+// length in shape 0 (the slots with launches of their own are not in it).
+int batch_class(const eb2_server* s) { return shape_class(s->nbatch0); }
+
 // Switch the work list to tile shape `shape`.
 int use_shape(eb2_server* s, int shape) {
     if (shape == s->shape && !s->dirty) return EB2_OK;
@@ -308,13 +356,13 @@ int use_shape(eb2_server* s, int shape) {
 }
 
 // One graph launch (kStepsPerGraph batch steps) with the tuned launch shape.
-// The autotuner times, per batch-shape class (log2 of the work-list length in
-// tile shape 0), every tile shape of the server's form and, per tile shape,
+// The autotuner times, per batch-shape class (log2 of the batched work-list
+// length in tile shape 0), every tile shape of the server's form and, per tile shape,
 // persistent grids of 1..CTAS CTAs per SM smaller than the work list and one
 // CTA per work item; the fastest is kept for the class.
 int launch_steps(eb2_server* s) {
     const int prec = s->precision == EB2_MIXED ? 1 : 0;
-    const int cls = shape_class(s->nwork0);
+    const int cls = batch_class(s);
     auto it = s->tuned.find(cls);
     if (it == s->tuned.end()) {
         HostTimer timer(s->tune_s);
@@ -329,8 +377,9 @@ int launch_steps(eb2_server* s) {
             // one CTA per work item over 2^k CTAs covers every work-list length
             // of this class in this shape (an 8-row tile shape has up to twice
             // the tiles of shape 0, a 32-row one at most as many)
-            const int each_grid = 1 << (cls + (batch_shape_tile_x(prec, sh) <
-                                               batch_shape_tile_x(prec, 0) ? 1 : 0));
+            const int each_grid = 1 << (shape_class(s->nbatch0) +
+                                        (batch_shape_tile_x(prec, sh) <
+                                         batch_shape_tile_x(prec, 0) ? 1 : 0));
             // persistent grids are tried in the default shape only: the trials
             // cost host time (a capture each) and progress at a worse rate
             std::vector<int> keys;
@@ -362,7 +411,6 @@ int launch_steps(eb2_server* s) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         s->tuned[cls] = best;
-        s->tuned_ms[cls] = best_ms;
         return use_shape(s, best >> 24);
     }
     if (int r = use_shape(s, it->second >> 24)) return r;
@@ -464,6 +512,12 @@ int eb2_server_create(eb2_server** out, int device, int max_slots,
         cudaMalloc(&s->d_active, (size_t)max_slots * sizeof(int)) ||
         cudaMallocHost(&s->h_active, (size_t)max_slots * sizeof(int)))
         return bail(fail(EB2_ENOMEM, "server allocation failed"));
+    if (cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming))
+        return bail(fail(EB2_ECUDA, "server events"));
+    for (int j = 0; j < eb2_server::kSide; j++)
+        if (cudaStreamCreateWithFlags(&s->side[j], cudaStreamNonBlocking) ||
+            cudaEventCreateWithFlags(&s->join[j], cudaEventDisableTiming))
+            return bail(fail(EB2_ECUDA, "server streams"));
     memset(s->h_desc, 0, (size_t)max_slots * sizeof(SlotDesc));
     if (cudaMemsetAsync(s->d_ctrl, 0, (size_t)max_slots * sizeof(Ctrl), s->stream) ||
         cudaMemcpyAsync(s->d_desc, s->h_desc, (size_t)max_slots * sizeof(SlotDesc),
@@ -481,6 +535,12 @@ int eb2_server_destroy(eb2_server* s) {
     destroy_graphs(s);
     if (s->busy0) cudaEventDestroy(s->busy0);
     if (s->busy1) cudaEventDestroy(s->busy1);
+    for (int j = 0; j < eb2_server::kSide; j++) {
+        if (s->side[j]) cudaStreamSynchronize(s->side[j]);
+        if (s->side[j]) cudaStreamDestroy(s->side[j]);
+        if (s->join[j]) cudaEventDestroy(s->join[j]);
+    }
+    if (s->fork) cudaEventDestroy(s->fork);
     for (auto& sl : s->slots)
         if (sl.used) {
             cudaFree(sl.u);
@@ -593,6 +653,8 @@ int eb2_server_submit(eb2_server* s, const eb2_request* r, long long* id) {
     sd.tiles_x = (r->ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y;
     for (int k = 0; k < s->nshapes; k++) sd.ntiles[k] = slot_tiles(r->nx, r->ny, prec, k);
     sd.ncells = r->nx * r->ny;
+    sd.npartials = prec ? sd.tiles_x * ((r->nx + MIXED_PARTIAL_ROWS - 1) / MIXED_PARTIAL_ROWS)
+                        : sd.ntiles[0];
     CKU(launch_init(sl.u, sd.grid, sd.gas, d, s->stream));
     // control block and first CFL step, as eb2_run starts a solve
     const double cfl = r->cfl > 0.0 ? r->cfl : 0.5;
@@ -622,18 +684,24 @@ int eb2_server_step(eb2_server* s, int ngraphs, int* nfinished) {
     if (s->dirty)
         if (int r = rebuild(s)) return r;
     if (nfinished) *nfinished = 0;
-    if (s->nwork == 0) return EB2_OK;
+    if (s->nwork == 0 && s->own.empty()) return EB2_OK;  // no active slot
     if (!s->busy0) {
         CKS(cudaEventCreate(&s->busy0));
         CKS(cudaEventCreate(&s->busy1));
     }
     CKS(cudaEventRecord(s->busy0, s->stream));
+    const long long launched = s->graph_launches;
     for (int k = 0; k < ngraphs; k++)
         if (int r = launch_steps(s)) return r;
     CKS(cudaEventRecord(s->busy1, s->stream));
     int r = harvest(s, nfinished);  // synchronizes the stream
     float ms = 0.0f;
-    if (!r && cudaEventElapsedTime(&ms, s->busy0, s->busy1) == cudaSuccess) s->busy_ms += ms;
+    if (!r && cudaEventElapsedTime(&ms, s->busy0, s->busy1) == cudaSuccess) {
+        s->busy_ms += ms;
+        // (not when autotuner trials ran in this call)
+        if (s->graph_launches - launched == ngraphs && ngraphs > 0)
+            s->last_graph_ms = ms / (float)ngraphs;
+    }
     return r;
 }
 
@@ -743,11 +811,11 @@ int eb2_server_run_trace(eb2_server* s, const eb2_request* reqs, const double* a
         int nf = 0;
         // enough graphs per call that the GPU works ~2 ms between the host's
         // harvests (a small batch's graph takes a fraction of that, and the
-        // host's admission and retirement work would otherwise leave it idle)
+        // host's admission and retirement work would otherwise leave it idle),
+        // from the device time per graph of the last call
         int ngraphs = 1;
-        auto tm = s->tuned_ms.find(shape_class(s->nwork0));
-        if (!s->dirty && tm != s->tuned_ms.end() && tm->second > 0.0f)
-            ngraphs = std::max(1, std::min(16, (int)(2.0f / tm->second)));
+        if (s->last_graph_ms > 0.0f)
+            ngraphs = std::max(1, std::min(16, (int)(2.0f / s->last_graph_ms)));
         if (int rc = eb2_server_step(s, ngraphs, &nf)) return rc;
         if (!nf) continue;
         const double tf = now_s() - t0;

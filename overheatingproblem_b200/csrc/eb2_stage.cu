@@ -20,10 +20,8 @@ cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s) {
     }
 }
 
-int mixed_solve_tile_x();  // eb2_stage_mixed.cu
-
 int stage_blocks(const Grid& g, bool mixed) {
-    const int tx = mixed ? mixed_solve_tile_x() : FP64_TILE_X;
+    const int tx = mixed ? MIXED_PARTIAL_ROWS : FP64_TILE_X;
     return ((g.ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y) * ((g.nx + tx - 1) / tx);
 }
 

@@ -21,7 +21,6 @@ static cudaError_t by_flux(const StageArgs& a, cudaStream_t s) {
 
 // Tile rows of the single-solve mixed stage (its partials hold one triple per
 // tile).
-int mixed_solve_tile_x() { return mixstage::SolveShape::TX; }
 
 cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s) {
     // the mixed form implements the characteristic WENO5 reconstruction only

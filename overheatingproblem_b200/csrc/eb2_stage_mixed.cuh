@@ -245,7 +245,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     float4* sU = sFy + YS;
     float4* sP = sU + FS;
     float2* sH = reinterpret_cast<float2*>(sP + PS);
-    __shared__ double red[3][NT / 32];
+    // per tile row: max |u|+a, max |v|+a and the sum of p (the CFL partials)
+    __shared__ double rowred[3][TX];
 
     const int rows = a.grid.rows, cols = a.grid.cols;
     const size_t plane = (size_t)rows * cols;
@@ -339,8 +340,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
     const double dt = ctrl->dt;
     const double idx = a.grid.inv_dx, idy = a.grid.inv_dy;
     const double grav = a.num.gravity;
-    double mx = 0.0, my = 0.0, ps = 0.0;
     constexpr int NC = TX * TY / NT;
+    // the CFL partials of this thread's cells (zero outside the domain)
+    double cmx[NC], cmy[NC], cps[NC];
     double xs[NC][4], ys[NC][4];
 #pragma unroll
     for (int t = 0; t < NC; t++) {
@@ -360,6 +362,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
         const int e = threadIdx.x + t * NT;
         const int rr = e / TY, cc = e - rr * TY;
         const int i = i0 + rr, j = j0 + cc;
+        cmx[t] = cmy[t] = cps[t] = 0.0;
         if (i >= rows - GC || j >= cols - GC) continue;
         const size_t o = (size_t)i * cols + j;
         const double* x = xs[t];
@@ -396,40 +399,52 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int ti, int tj, i
             double uu = out[1] * ir, vv = out[2] * ir;
             double p = (out[3] - 0.5 * rho * (uu * uu + vv * vv)) * g.gm1;
             double c = sqrt(g.gamma * p * ir);
-            double lx = fabs(uu) + c, ly = fabs(vv) + c;
-            if (lx > mx) mx = lx;
-            if (ly > my) my = ly;
-            ps += p;
+            cmx[t] = fabs(uu) + c;
+            cmy[t] = fabs(vv) + c;
+            cps[t] = p;
         }
     }
 
     unsigned wst = __reduce_or_sync(0xffffffffu, st);
     if (wst && (threadIdx.x & 31) == 0) atomicOr(&ctrl->status, wst);
     if (a.partials) {
+        // A warp holds one tile row per t (lane = column), reduced over a fixed
+        // lane tree; then one partial triple per 8-row block, its rows summed
+        // in order.  So the partials, and the mean pressure summed from them,
+        // are the same bits in every tile shape.
+        const int w = threadIdx.x >> 5;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            double ox = __shfl_down_sync(0xffffffffu, mx, off);
-            double oy = __shfl_down_sync(0xffffffffu, my, off);
-            double op = __shfl_down_sync(0xffffffffu, ps, off);
-            if (ox > mx) mx = ox;
-            if (oy > my) my = oy;
-            ps += op;
-        }
-        int w = threadIdx.x >> 5;
-        if ((threadIdx.x & 31) == 0) {
-            red[0][w] = mx;
-            red[1][w] = my;
-            red[2][w] = ps;
+        for (int t = 0; t < NC; t++) {
+            double x = cmx[t], y = cmy[t], p = cps[t];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ox = __shfl_down_sync(0xffffffffu, x, off);
+                const double oy = __shfl_down_sync(0xffffffffu, y, off);
+                const double op = __shfl_down_sync(0xffffffffu, p, off);
+                if (ox > x) x = ox;
+                if (oy > y) y = oy;
+                p += op;
+            }
+            if ((threadIdx.x & 31) == 0) {
+                const int row = w + t * (NT / 32);
+                rowred[0][row] = x;
+                rowred[1][row] = y;
+                rowred[2][row] = p;
+            }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        constexpr int NB = TX / MIXED_PARTIAL_ROWS;
+        const int k = threadIdx.x;
+        if (k < NB && ti * TX + k * MIXED_PARTIAL_ROWS < a.grid.nx) {
             double bx = 0.0, by = 0.0, bp = 0.0;
-            for (int q = 0; q < NT / 32; q++) {
-                if (red[0][q] > bx) bx = red[0][q];
-                if (red[1][q] > by) by = red[1][q];
-                bp += red[2][q];
+#pragma unroll
+            for (int r = 0; r < MIXED_PARTIAL_ROWS; r++) {
+                const int row = k * MIXED_PARTIAL_ROWS + r;
+                if (rowred[0][row] > bx) bx = rowred[0][row];
+                if (rowred[1][row] > by) by = rowred[1][row];
+                bp += rowred[2][row];
             }
-            size_t b = (size_t)ti * tiles_x + tj;
+            const size_t b = (size_t)(ti * (TX / MIXED_PARTIAL_ROWS) + k) * tiles_x + tj;
             a.partials[3 * b + 0] = bx;
             a.partials[3 * b + 1] = by;
             a.partials[3 * b + 2] = bp;

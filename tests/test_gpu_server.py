@@ -70,6 +70,42 @@ def test_result_same_alone_and_in_the_mix(gpu, precision, scheme):
         assert np.all(np.isfinite(a))
 
 
+def test_slot_that_fills_the_gpu_has_its_own_launch(gpu):
+    """A mixed slot with more tiles than the GPU holds CTAs (768^2: 1152 tiles
+    of 16 x 32) runs as a stage launch of its own beside the batched launch of
+    the small slots; its result and theirs stay the bits of single-solve runs."""
+    from overheatingproblem_b200.server import Request, Server
+    L = gpu.lib
+    rng = np.random.default_rng(5)
+    reqs = [Request(L.CASE_FOUR_QUADRANT, 768, 768, q=fq_states(rng), tmax=0.02),
+            Request(L.CASE_FOUR_QUADRANT, 64, 64, q=fq_states(rng), tmax=0.03),
+            Request(L.CASE_WALL_HEATING, 96, 96, q=[1.3], ly=1.0, tmax=0.025)]
+    with Server(precision=L.MIXED, scheme=2) as srv:
+        got = srv.run_trace(reqs, np.zeros(len(reqs)), keep_results=True)["results"]
+    for i, req in enumerate(reqs):
+        ctx = run_alone_ctx(gpu, req, L.MIXED)
+        a, c = (x[:, 4:-4, 4:-4] for x in (got[i], ctx))
+        assert np.all(np.isfinite(c)), i
+        assert np.array_equal(a.view(np.int64), c.view(np.int64)), i
+
+
+def test_reused_slot_with_its_own_launch(gpu):
+    """Two large mixed requests of different sizes through one slot, one after
+    the other: the second reuses the slot index with a grid and buffers of its
+    own, and its launch must follow them (same bits as a single-solve run)."""
+    from overheatingproblem_b200.server import Request, Server
+    L = gpu.lib
+    rng = np.random.default_rng(9)
+    reqs = [Request(L.CASE_FOUR_QUADRANT, 768, 768, q=fq_states(rng), tmax=0.01),
+            Request(L.CASE_FOUR_QUADRANT, 896, 896, q=fq_states(rng), tmax=0.015)]
+    with Server(precision=L.MIXED, scheme=2, max_slots=1) as srv:
+        got = srv.run_trace(reqs, np.zeros(len(reqs)), keep_results=True)["results"]
+    for i, req in enumerate(reqs):
+        ctx = run_alone_ctx(gpu, req, L.MIXED)
+        a, c = (x[:, 4:-4, 4:-4] for x in (got[i], ctx))
+        assert np.array_equal(a.view(np.int64), c.view(np.int64)), i
+
+
 def test_admission_by_budget_and_retirement(gpu):
     from overheatingproblem_b200.server import Request, Server
     L = gpu.lib
