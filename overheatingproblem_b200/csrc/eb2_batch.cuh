@@ -23,7 +23,7 @@ struct SlotDesc {
     double* u;            // state
     double* u1;           // stage 1 output
     double* u2;           // stage 2 output
-    double* partials;     // wave-speed partials, one triple per tile
+    double* partials;     // CFL partials (npartials triples)
     Ctrl* ctrl;           // control block of this solve
     Grid grid;
     Gas gas;

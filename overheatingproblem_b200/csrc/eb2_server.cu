@@ -10,6 +10,8 @@
 // retirement only rewrite the work list and descriptor arrays, so the graphs
 // are reused; a graph is captured per persistent-grid size, and the size is
 // picked per batch-shape class by timing the candidates (the autotuner).
+// A mixed slot that fills the GPU by itself gets a stage launch of its own in
+// the graph, forked beside the batched launch of the other slots.
 // Every slot has its own time, CFL step and final time.
 #include <algorithm>
 #include <cstdarg>
@@ -71,7 +73,8 @@ int slot_tiles(int nx, int ny, int precision, int shape) {
     return ((ny + STAGE_TILE_Y - 1) / STAGE_TILE_Y) * ((nx + tx - 1) / tx);
 }
 
-// Partials of a slot: one triple per tile in the shape with the most tiles.
+// Partials of a slot: one triple per tile in the shape with the most tiles (for
+// the mixed form the 8-row shape, whose tiles are the 8 x 32 partial blocks).
 int slot_partials(int nx, int ny, int precision) {
     int n = 296;
     for (int k = 0; k < batch_shapes(precision); k++)
