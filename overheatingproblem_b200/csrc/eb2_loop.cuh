@@ -132,7 +132,24 @@ __device__ __forceinline__ void finalize_body(Ctrl* c, const double* __restrict_
                                               int nblocks, int ncells, int mode, double* red) {
     if (mode == 2 && !c->active) return;
     double mx = 0.0, my = 0.0, ps = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    // each thread combines partials b, b + blockDim.x, ... in that order; the
+    // loads of eight of them are issued before they are combined
+    const int step = blockDim.x;
+    int b = threadIdx.x;
+    for (; b + 7 * step < nblocks; b += 8 * step) {
+        double a[8][3];
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) a[u][k] = partials[3 * (b + u * step) + k];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            if (a[u][0] > mx) mx = a[u][0];
+            if (a[u][1] > my) my = a[u][1];
+            ps += a[u][2];
+        }
+    }
+    for (; b < nblocks; b += step) {
         double a0 = partials[3 * b], a1 = partials[3 * b + 1];
         if (a0 > mx) mx = a0;
         if (a1 > my) my = a1;
