@@ -190,7 +190,7 @@ cudaError_t launch_wave_partials(const double* u, const Grid& g, const Gas& gas,
 }
 
 // End-of-step reduction and time bookkeeping (body in eb2_loop.cuh).
-__global__ void k_finalize(Ctrl* c, const double* __restrict__ partials, int nblocks,
+__global__ void __launch_bounds__(FINALIZE_THREADS) k_finalize(Ctrl* c, const double* __restrict__ partials, int nblocks,
                            int ncells, int mode) {
     __shared__ double red[96];
     finalize_body(c, partials, nblocks, ncells, mode, red);
@@ -198,7 +198,7 @@ __global__ void k_finalize(Ctrl* c, const double* __restrict__ partials, int nbl
 
 cudaError_t launch_finalize(Ctrl* ctrl, const double* partials, int nblocks, int ncells,
                             int mode, cudaStream_t s) {
-    k_finalize<<<1, NT, 0, s>>>(ctrl, partials, nblocks, ncells, mode);
+    k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(ctrl, partials, nblocks, ncells, mode);
     return cudaGetLastError();
 }
 

@@ -109,7 +109,7 @@ cudaError_t launch_bc_batch(const BatchLaunch& b, int stage, cudaStream_t s) {
 }
 
 // End of a step for every active slot: one block per slot.
-__global__ void k_finalize_batch(const SlotDesc* __restrict__ slots, const int* __restrict__ act,
+__global__ void __launch_bounds__(FINALIZE_THREADS) k_finalize_batch(const SlotDesc* __restrict__ slots, const int* __restrict__ act,
                                  const int* __restrict__ nact) {
     __shared__ double red[96];
     if ((int)blockIdx.x >= *nact) return;
@@ -119,7 +119,7 @@ __global__ void k_finalize_batch(const SlotDesc* __restrict__ slots, const int* 
 }
 
 cudaError_t launch_finalize_batch(const BatchLaunch& b, cudaStream_t s) {
-    k_finalize_batch<<<b.active_grid, 256, 0, s>>>(b.slots, b.active, b.nactive);
+    k_finalize_batch<<<b.active_grid, FINALIZE_THREADS, 0, s>>>(b.slots, b.active, b.nactive);
     return cudaGetLastError();
 }
 

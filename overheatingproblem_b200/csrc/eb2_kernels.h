@@ -41,6 +41,9 @@ constexpr int FP64_TILE_X = 15, MIXED_TILE_X = 16, STAGE_TILE_Y = 32;
 // The mixed stage kernels write one CFL partial triple per 8-row x 32-column
 // block, whatever their tile shape (each tile shape's rows are a multiple of 8).
 constexpr int MIXED_PARTIAL_ROWS = 8;
+// Threads of the end-of-step reduction block (single solves and the server
+// alike, so that both sum the partials in the same order).
+constexpr int FINALIZE_THREADS = 1024;
 // Blocks of one stage launch of the given form, and the most of either form
 // (the size of a partials buffer).
 int stage_blocks(const Grid& g, bool mixed);
